@@ -1,0 +1,65 @@
+"""Build libhb_gpu.so in-tree: CUDA kernels for sm_100a (nvcc) + host client code (g++).
+
+Usage: python -m hasteboots_b200.build [--force]
+"""
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libhb_gpu.so")
+BUILD = os.path.join(HERE, "_build")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+CXX = os.environ.get("CXX", "g++")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = ["hb_api.cu"]
+CPP_SOURCES = ["hb_client.cpp"]
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [
+        os.path.join(HERE, "..", "include", "hb_gpu.h")]
+
+
+def up_to_date():
+    if not os.path.exists(OUT):
+        return False
+    t = os.path.getmtime(OUT)
+    return all(os.path.getmtime(s) <= t for s in _sources())
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(force=False, verbose_ptxas=False):
+    if not force and up_to_date():
+        return OUT
+    os.makedirs(BUILD, exist_ok=True)
+    objs = []
+    for src in CU_SOURCES:
+        obj = os.path.join(BUILD, src + ".o")
+        cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+               "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose_ptxas:
+            cmd.insert(1, "-Xptxas=-v")
+        _run(cmd)
+        objs.append(obj)
+    for src in CPP_SOURCES:
+        obj = os.path.join(BUILD, src + ".o")
+        _run([CXX, "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-fno-fast-math",
+              "-I", "/usr/local/cuda/include", "-c", os.path.join(CSRC, src), "-o", obj])
+        objs.append(obj)
+    tmp = OUT + ".tmp"
+    _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-lpthread"])
+    os.replace(tmp, OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv)

@@ -1,0 +1,420 @@
+// hb_client.cpp -- host-side parameters, key generation, encryption and decryption
+// (the tfhe crate's KeyGen / Encryptor / Decryptor and Evaluator::new key material).
+//
+// Seeded key convention: every random value is drawn from a counter PRG
+//   rand(seed, stream, ctr) = mix(mix(seed + g) ^ mix(stream ^ c) + ctr * g)
+// (mix = splitmix64 finaliser), so key generation parallelises over polynomials and is identical on
+// every host. Streams: (tag, i, part, j, which) packed into 64 bits. Distributions follow the
+// reference: binary LWE key (algebra/src/utils/sample.rs:6-27), ternary ring key {0,0,1,-1}[r&3]
+// (sample.rs:30-51), uniform field elements, and the discrete Gaussian of
+// FieldDiscreteGaussianSampler (algebra/src/random.rs:156-171: N(0, sigma), reject |x| >= 6 sigma,
+// round half away from zero, negative r -> Q - |r|) with normal deviates from the Marsaglia polar
+// method and a logarithm built from IEEE-exact operations.
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "../../include/hb_gpu.h"
+#include "hb_field.cuh"
+
+namespace {
+
+using u64 = uint64_t;
+using u128 = unsigned __int128;
+
+// ---- field helpers (host, canonical) ----
+template <class F>
+struct HostField {
+  using W = typename F::W;
+  static W add(W a, W b) {
+    u64 s = (u64)a + b;
+    if (sizeof(W) == 8) {
+      // a, b < P < 2^64: detect wrap
+      W r = (W)s;
+      if (r < a || r >= F::P) r = (W)(r - F::P);
+      return r;
+    }
+    return (W)(s >= F::P ? s - F::P : s);
+  }
+  static W sub(W a, W b) { return a >= b ? (W)(a - b) : (W)(a + (F::P - b)); }
+  static W mul(W a, W b) { return (W)(((u128)a * b) % F::P); }
+  static W neg(W a) { return a == 0 ? 0 : (W)(F::P - a); }
+};
+
+// ---- PRG ----
+inline u64 mix(u64 z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+inline u64 rnd(u64 seed, u64 stream, u64 ctr) {
+  const u64 key = mix(seed + 0x9E3779B97F4A7C15ULL) ^ mix(stream ^ 0xD1B54A32D192ED03ULL);
+  return mix(key + ctr * 0x9E3779B97F4A7C15ULL);
+}
+constexpr u64 kTagLweSk = 1, kTagRingSk = 2, kTagBsk = 3, kTagKsk = 4, kTagEnc = 5;
+inline u64 stream_of(u64 tag, u64 i, u64 part, u64 j, u64 which) {
+  return (tag << 56) | ((i & 0xFFFFFFFFULL) << 24) | ((part & 0xFF) << 16) | ((j & 0xFF) << 8) |
+         (which & 0xFF);
+}
+
+// ln(s), s in (0, 1]: s = m 2^e with m in [1/sqrt2, sqrt2), ln s = e ln2 + 2 atanh((m-1)/(m+1)),
+// atanh by its odd power series (24 terms; |y| <= 0.1716).
+double log_unit(double s) {
+  int e;
+  double m = std::frexp(s, &e);
+  if (m < 0.70710678118654752440) {
+    m = m * 2.0;
+    e = e - 1;
+  }
+  const double y = (m - 1.0) / (m + 1.0);
+  const double y2 = y * y;
+  double acc = 0.0;
+  double pw = y;
+  for (int k = 0; k < 24; ++k) {
+    acc = acc + pw / (double)(2 * k + 1);
+    pw = pw * y2;
+  }
+  return 2.0 * acc + (double)e * 0.693147180559945309417232121458;
+}
+
+inline double to_unit(u64 r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
+
+template <class F>
+typename F::W sample_gauss(u64 seed, u64 stream, u64 coeff, double sigma) {
+  const double bound = sigma * 6.0;
+  for (u64 attempt = 0;; ++attempt) {
+    const u64 ctr = (coeff << 20) | (attempt << 1);
+    const double u = 2.0 * to_unit(rnd(seed, stream, ctr)) - 1.0;
+    const double v = 2.0 * to_unit(rnd(seed, stream, ctr | 1)) - 1.0;
+    const double s = u * u + v * v;
+    if (!(s > 0.0 && s < 1.0)) continue;
+    const double z = u * std::sqrt(-2.0 * log_unit(s) / s);
+    const double val = sigma * z;
+    if (std::fabs(val) >= bound) continue;
+    const double r = std::round(val);
+    if (r < 0.0) return (typename F::W)((u64)F::P - (u64)(-r));
+    return (typename F::W)(u64)r;
+  }
+}
+
+template <class F>
+inline typename F::W sample_uniform(u64 seed, u64 stream, u64 k) {
+  return (typename F::W)(rnd(seed, stream, k) % (u64)F::P);
+}
+
+// ---- host negacyclic multiplication for key generation (radix-2, twisted cyclic NTT) ----
+template <class F>
+struct HostRing {
+  using W = typename F::W;
+  using H = HostField<F>;
+  uint32_t n, logn;
+  std::vector<W> twist, untwist, roots, iroots;
+  std::vector<uint32_t> rev;
+  W ninv;
+
+  explicit HostRing(uint32_t logn_) : n(1u << logn_), logn(logn_) {
+    const u64 order = (u64)F::P - 1;
+    W psi = 0;
+    for (W g = 2; g < 64 && !psi; ++g) {
+      W c = hb::host_powmod<F>(g, order / (2ull * n));
+      if (hb::host_powmod<F>(c, n) == (W)(F::P - 1)) psi = c;
+    }
+    const W psi_inv = hb::host_powmod<F>(psi, (u64)F::P - 2);
+    twist.resize(n);
+    untwist.resize(n);
+    W a = 1, b = 1;
+    ninv = hb::host_powmod<F>((W)n, (u64)F::P - 2);
+    for (uint32_t i = 0; i < n; ++i) {
+      twist[i] = a;
+      untwist[i] = H::mul(b, ninv);
+      a = H::mul(a, psi);
+      b = H::mul(b, psi_inv);
+    }
+    const W w = H::mul(psi, psi), wi = H::mul(psi_inv, psi_inv);
+    roots.assign(n, 0);
+    iroots.assign(n, 0);
+    for (uint32_t half = 1; half < n; half <<= 1) {
+      const W step = hb::host_powmod<F>(w, n / (2 * half));
+      const W istep = hb::host_powmod<F>(wi, n / (2 * half));
+      W x = 1, y = 1;
+      for (uint32_t j = 0; j < half; ++j) {
+        roots[half + j] = x;
+        iroots[half + j] = y;
+        x = H::mul(x, step);
+        y = H::mul(y, istep);
+      }
+    }
+    rev.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      uint32_t r = 0;
+      for (uint32_t b2 = 0; b2 < logn; ++b2) r |= ((i >> b2) & 1) << (logn - 1 - b2);
+      rev[i] = r;
+    }
+  }
+  void dft(W *a, const std::vector<W> &rt) const {
+    for (uint32_t i = 0; i < n; ++i)
+      if (i < rev[i]) std::swap(a[i], a[rev[i]]);
+    for (uint32_t half = 1; half < n; half <<= 1)
+      for (uint32_t i = 0; i < n; i += 2 * half)
+        for (uint32_t j = 0; j < half; ++j) {
+          const W u = a[i + j], v = H::mul(a[i + j + half], rt[half + j]);
+          a[i + j] = H::add(u, v);
+          a[i + j + half] = H::sub(u, v);
+        }
+  }
+  void to_eval(W *a) const {
+    for (uint32_t i = 0; i < n; ++i) a[i] = H::mul(a[i], twist[i]);
+    dft(a, roots);
+  }
+  void to_coeff(W *a) const {
+    dft(a, iroots);
+    for (uint32_t i = 0; i < n; ++i) a[i] = H::mul(a[i], untwist[i]);
+  }
+  // out = x * y where y_eval is y in evaluation form
+  void mul(const W *x, const W *y_eval, W *out) const {
+    std::vector<W> t(x, x + n);
+    to_eval(t.data());
+    for (uint32_t i = 0; i < n; ++i) t[i] = H::mul(t[i], y_eval[i]);
+    to_coeff(t.data());
+    std::memcpy(out, t.data(), sizeof(W) * n);
+  }
+};
+
+bool check_params(const hb_params *p) {
+  if (!p) return false;
+  if (p->field_id != HB_FIELD_BABYBEAR && p->field_id != HB_FIELD_GOLDILOCKS) return false;
+  const uint32_t N = p->ring_dim;
+  if (N < 4 || N > 4096 || (N & (N - 1))) return false;
+  if (p->lwe_dim == 0 || p->lwe_dim > N) return false;
+  uint32_t np2 = 1;
+  while (np2 < p->lwe_dim) np2 <<= 1;
+  if (np2 != N) return false;  // the RLWE key switch of the reference sets (next_pow2(n) == N)
+  // Parameters::new: 2N | Q - 1 (fhe_core/src/parameter.rs:131-138)
+  const u64 q = p->field_id == HB_FIELD_GOLDILOCKS ? hb::Goldilocks::P : hb::BabyBear::P;
+  if ((q - 1) % (2ull * N) != 0) return false;
+  const uint32_t qbits = p->field_id == HB_FIELD_GOLDILOCKS ? 64 : 31;
+  if (p->br_bits == 0 || p->br_bits > 16 || p->ks_bits == 0 || p->ks_bits > 16) return false;
+  if (p->br_len != (qbits + p->br_bits - 1) / p->br_bits) return false;
+  if (p->ks_len != (qbits + p->ks_bits - 1) / p->ks_bits) return false;
+  if (!(p->lwe_noise_std >= 0) || !(p->ring_noise_std >= 0) || !(p->ks_noise_std >= 0)) return false;
+  return true;
+}
+
+template <class F>
+void keygen_impl(const hb_params *p, u64 seed, typename F::W *lwe_sk, typename F::W *ring_sk,
+                 typename F::W *bsk, typename F::W *ksk, int threads) {
+  using W = typename F::W;
+  using H = HostField<F>;
+  const uint32_t N = p->ring_dim, n = p->lwe_dim, L = p->br_len;
+  for (uint32_t i = 0; i < n; ++i) lwe_sk[i] = (W)(rnd(seed, stream_of(kTagLweSk, 0, 0, 0, 0), i) & 1);
+  static const int kTern[4] = {0, 0, 1, -1};
+  for (uint32_t k = 0; k < N; ++k) {
+    const u64 r = rnd(seed, stream_of(kTagRingSk, 0, 0, 0, 0), k);
+    if (p->ring_ternary) {
+      const int v = kTern[r & 3];
+      ring_sk[k] = v < 0 ? (W)(F::P - 1) : (W)v;
+    } else {
+      ring_sk[k] = (W)(r & 1);
+    }
+  }
+  if (!bsk) return;
+  uint32_t logn = 0;
+  while ((1u << logn) < N) ++logn;
+  HostRing<F> ring(logn);
+  std::vector<W> z_eval(ring_sk, ring_sk + N);
+  ring.to_eval(z_eval.data());
+
+  // One RLWE zero sample: a uniform, b = a*key + e.
+  auto zero_sample = [&](const W *key_eval, u64 sa, u64 se, double sigma, W *a, W *b) {
+    for (uint32_t k = 0; k < N; ++k) a[k] = sample_uniform<F>(seed, sa, k);
+    ring.mul(a, key_eval, b);
+    for (uint32_t k = 0; k < N; ++k) b[k] = H::add(b[k], sample_gauss<F>(seed, se, k, sigma));
+  };
+
+  // BSK: per LWE key bit an NTTRGSW zero sample (s_i = 0) or one sample (s_i = 1)
+  // (lattice/src/rgsw.rs:343-395): c_neg_s_m rows (a + B^j, b) / c_m rows (a, b + B^j).
+  const size_t rows_total = (size_t)n * 2 * L;
+  std::atomic<size_t> next{0};
+  auto worker = [&] {
+    for (size_t q; (q = next.fetch_add(1)) < rows_total;) {
+      const uint32_t i = (uint32_t)(q / (2 * L));
+      const uint32_t part = (uint32_t)((q / L) % 2);
+      const uint32_t j = (uint32_t)(q % L);
+      W *a = bsk + q * 2 * N;
+      W *b = a + N;
+      zero_sample(z_eval.data(), stream_of(kTagBsk, i, part, j, 0), stream_of(kTagBsk, i, part, j, 1),
+                  p->ring_noise_std, a, b);
+      if (lwe_sk[i]) {
+        const W bj = (W)((u64)1 << (j * p->br_bits));
+        if (part == 0)
+          a[0] = H::add(a[0], bj);
+        else
+          b[0] = H::add(b[0], bj);
+      }
+    }
+  };
+  const int nt = std::max(1, threads);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
+  for (auto &th : pool) th.join();
+
+  // KSK rows j: zero samples under the extended LWE key, plus z * B_ks^j on b
+  // (fhe_core/src/key_switch/rlwe.rs:57-78).
+  std::vector<W> s_eval(N, 0);
+  for (uint32_t i = 0; i < n; ++i) s_eval[i] = lwe_sk[i];
+  ring.to_eval(s_eval.data());
+  std::vector<W> zpow(ring_sk, ring_sk + N);
+  const W bks = (W)(1u << p->ks_bits);
+  for (uint32_t j = 0; j < p->ks_len; ++j) {
+    W *a = ksk + (size_t)j * 2 * N;
+    W *b = a + N;
+    zero_sample(s_eval.data(), stream_of(kTagKsk, 0, 0, j, 0), stream_of(kTagKsk, 0, 0, j, 1),
+                p->ks_noise_std, a, b);
+    for (uint32_t k = 0; k < N; ++k) b[k] = H::add(b[k], zpow[k]);
+    for (uint32_t k = 0; k < N; ++k) zpow[k] = H::mul(zpow[k], bks);
+  }
+}
+
+template <class F>
+u64 encode_msg(u64 m) {
+  const double q = (double)(u64)F::P;
+  return (u64)std::round((double)m * (q / 4.0));  // fhe_core/src/plaintext.rs:64-75, t = 4
+}
+template <class F>
+u64 decode_msg(u64 c) {
+  const double q = (double)(u64)F::P;
+  const u64 r = (u64)std::round((double)c * 4.0 / q);  // plaintext.rs:87-97
+  return r < 4 ? r : r - 4;
+}
+
+template <class F>
+void encrypt_impl(const hb_params *p, const typename F::W *sk, u64 seed, u64 index0,
+                  const uint8_t *bits, size_t count, typename F::W *out) {
+  using W = typename F::W;
+  using H = HostField<F>;
+  const uint32_t n = p->lwe_dim;
+  for (size_t c = 0; c < count; ++c) {
+    W *ct = out + c * (n + 1);
+    const u64 idx = index0 + c;
+    W dot = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      ct[i] = sample_uniform<F>(seed, stream_of(kTagEnc, idx, 0, 0, 0), i);
+      dot = H::add(dot, H::mul(ct[i], sk[i]));
+    }
+    const W e = sample_gauss<F>(seed, stream_of(kTagEnc, idx, 0, 0, 1), 0, p->lwe_noise_std);
+    ct[n] = H::add(H::add(dot, e), (W)encode_msg<F>(bits[c] & 1));
+  }
+}
+
+template <class F>
+void decrypt_impl(const hb_params *p, const typename F::W *sk, const typename F::W *in, size_t count,
+                  uint8_t *bits, uint64_t *noise) {
+  using W = typename F::W;
+  using H = HostField<F>;
+  const uint32_t n = p->lwe_dim;
+  for (size_t c = 0; c < count; ++c) {
+    const W *ct = in + c * (n + 1);
+    W dot = 0;
+    for (uint32_t i = 0; i < n; ++i) dot = H::add(dot, H::mul((W)(ct[i] % F::P), sk[i]));
+    const W pt = H::sub((W)(ct[n] % F::P), dot);
+    const u64 m = decode_msg<F>(pt);
+    if (bits) bits[c] = (uint8_t)m;
+    if (noise) {
+      const W fresh = (W)encode_msg<F>(m);
+      noise[c] = std::min<u64>(H::sub(pt, fresh), H::sub(fresh, pt));
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hb_params_preset(int preset, hb_params *out) {
+  if (!out) return HB_ERR_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  out->ring_dim = 1024;
+  out->lwe_dim = 728;
+  out->ring_ternary = 1;
+  out->ks_bits = 5;
+  if (preset == HB_PRESET_BABYBEAR_BINARY_128_BITS) {
+    out->field_id = HB_FIELD_BABYBEAR;
+    out->br_bits = 8;
+    out->br_len = 4;
+    out->ks_len = 7;
+    out->lwe_noise_std = 11000.0;
+    out->ring_noise_std = 41.9;
+    out->ks_noise_std = 11000.0;
+    return HB_OK;
+  }
+  if (preset == HB_PRESET_GOLDILOCKS_BINARY_128_BITS || preset == HB_PRESET_ZAMA_BINARY_128_BITS) {
+    const bool zama = preset == HB_PRESET_ZAMA_BINARY_128_BITS;
+    out->field_id = HB_FIELD_GOLDILOCKS;
+    out->br_bits = zama ? 5 : 8;
+    out->br_len = zama ? 13 : 8;
+    out->ks_len = 13;
+    out->lwe_noise_std = 2.9 * (double)(1ULL << 45);
+    out->ring_noise_std = 2.3 * (double)(1ULL << 37);
+    out->ks_noise_std = 2.9 * (double)(1ULL << 45);
+    return HB_OK;
+  }
+  return HB_ERR_INVALID;
+}
+
+int hb_params_validate(const hb_params *p) { return check_params(p) ? HB_OK : HB_ERR_INVALID; }
+
+int hb_params_sizes(const hb_params *p, size_t *lwe_sk, size_t *ring_sk, size_t *bsk, size_t *ksk,
+                    size_t *lwe) {
+  if (!check_params(p)) return HB_ERR_INVALID;
+  const size_t N = p->ring_dim, n = p->lwe_dim;
+  if (lwe_sk) *lwe_sk = n;
+  if (ring_sk) *ring_sk = N;
+  if (bsk) *bsk = n * 2 * p->br_len * 2 * N;
+  if (ksk) *ksk = (size_t)p->ks_len * 2 * N;
+  if (lwe) *lwe = n + 1;
+  return HB_OK;
+}
+
+int hb_keygen(const hb_params *p, uint64_t seed, void *lwe_sk, void *ring_sk, void *bsk, void *ksk,
+              int threads) {
+  // bsk and ksk may both be NULL: only the secret keys are produced (KeyGen::generate_secret_key).
+  if (!check_params(p) || !lwe_sk || !ring_sk || (!bsk != !ksk)) return HB_ERR_INVALID;
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  if (p->field_id == HB_FIELD_GOLDILOCKS)
+    keygen_impl<hb::Goldilocks>(p, seed, (uint64_t *)lwe_sk, (uint64_t *)ring_sk, (uint64_t *)bsk,
+                                (uint64_t *)ksk, threads);
+  else
+    keygen_impl<hb::BabyBear>(p, seed, (uint32_t *)lwe_sk, (uint32_t *)ring_sk, (uint32_t *)bsk,
+                              (uint32_t *)ksk, threads);
+  return HB_OK;
+}
+
+int hb_encrypt(const hb_params *p, const void *lwe_sk, uint64_t seed, uint64_t index0,
+               const uint8_t *bits, size_t count, void *lwe_out) {
+  if (!check_params(p) || !lwe_sk || (count && (!bits || !lwe_out))) return HB_ERR_INVALID;
+  if (p->field_id == HB_FIELD_GOLDILOCKS)
+    encrypt_impl<hb::Goldilocks>(p, (const uint64_t *)lwe_sk, seed, index0, bits, count,
+                                 (uint64_t *)lwe_out);
+  else
+    encrypt_impl<hb::BabyBear>(p, (const uint32_t *)lwe_sk, seed, index0, bits, count,
+                               (uint32_t *)lwe_out);
+  return HB_OK;
+}
+
+int hb_decrypt(const hb_params *p, const void *lwe_sk, const void *lwe, size_t count,
+               uint8_t *bits_out, uint64_t *noise_out) {
+  if (!check_params(p) || !lwe_sk || (count && !lwe)) return HB_ERR_INVALID;
+  if (p->field_id == HB_FIELD_GOLDILOCKS)
+    decrypt_impl<hb::Goldilocks>(p, (const uint64_t *)lwe_sk, (const uint64_t *)lwe, count, bits_out,
+                                 noise_out);
+  else
+    decrypt_impl<hb::BabyBear>(p, (const uint32_t *)lwe_sk, (const uint32_t *)lwe, count, bits_out,
+                               noise_out);
+  return HB_OK;
+}
+
+}  // extern "C"

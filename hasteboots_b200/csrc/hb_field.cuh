@@ -1,0 +1,163 @@
+// hb_field.cuh -- Goldilocks and BabyBear arithmetic for sm_100a on the integer pipe.
+//
+// Goldilocks Q = 2^64 - 2^32 + 1 (algebra/src/modulus/goldilocks/mod.rs:9-11): 64x64->128 products
+// folded with 2^64 = 2^32 - 1 and 2^96 = -1 (mod Q); values may sit anywhere in [0, 2^64) and are
+// canonicalised only where a canonical value is observed (decomposition, outputs).
+// The accumulator additions and negations use the reference's exact u64 operations
+// (algebra/src/modulus/goldilocks/ops.rs:26-73) because a non-canonical accumulator word is
+// negated by `P - x` there, and bit-exact outputs must follow that.
+//
+// BabyBear Q = 2^31 - 2^27 + 1 (algebra/src/modulus/baby_bear/mod.rs:11): data words are canonical
+// residues; constants that multiply data (twiddles, keys) are stored premultiplied by R = 2^32 so a
+// Montgomery product returns a canonical residue of the plain product.
+#pragma once
+
+#include <cstdint>
+
+#ifndef HB_HD
+#ifdef __CUDACC__
+#define HB_HD __host__ __device__ __forceinline__
+#else
+#define HB_HD inline
+#endif
+#endif
+
+namespace hb {
+
+struct Goldilocks {
+  using W = uint64_t;
+  static constexpr W P = 0xFFFFFFFF00000001ULL;
+  static constexpr W EPS = 0xFFFFFFFFULL;  // 2^64 mod P
+  static constexpr int BITS = 64;
+  static constexpr int FIELD_ID = 1;
+
+  HB_HD static W canon(W x) { return x >= P ? x - P : x; }
+
+  // Fold a 128-bit value (lo + hi*2^64) to [0, 2^64).
+  HB_HD static W fold(W lo, W hi) {
+    const uint32_t hh = (uint32_t)(hi >> 32);
+    const uint32_t hl = (uint32_t)hi;
+    W t0 = lo - hh;
+    if (lo < hh) t0 -= EPS;
+    const W t1 = ((W)hl << 32) - hl;  // hl * (2^32 - 1)
+    W r = t0 + t1;
+    if (r < t1) r += EPS;
+    return r;
+  }
+  HB_HD static W mul_lazy(W a, W b) {
+#ifdef __CUDA_ARCH__
+    return fold(a * b, __umul64hi(a, b));
+#else
+    unsigned __int128 x = (unsigned __int128)a * b;
+    return fold((W)x, (W)(x >> 64));
+#endif
+  }
+  // Product with a canonical result.
+  HB_HD static W mul(W a, W b) { return canon(mul_lazy(a, b)); }
+  // Sum/difference where `b` is canonical (< P): one carry fix-up suffices.
+  HB_HD static W add_c(W a, W b) {
+    W s = a + b;
+    if (s < b) s += EPS;
+    return s;
+  }
+  HB_HD static W sub_c(W a, W b) {
+    W d = a - b;
+    if (a < b) d -= EPS;
+    return d;
+  }
+  // Sum/difference of arbitrary words: the reference's add_reduce / sub_reduce
+  // (algebra/src/modulus/goldilocks/ops.rs:26-57).
+  HB_HD static W add(W a, W b) {
+    W s = a + b;
+    W c = s < a ? EPS : 0;
+    W s2 = s + c;
+    if (s2 < c) s2 += EPS;
+    return s2;
+  }
+  HB_HD static W sub(W a, W b) {
+    W d = a - b;
+    W c = a < b ? EPS : 0;
+    W d2 = d - c;
+    if (d < c) d2 -= EPS;
+    return d2;
+  }
+  // neg_reduce (ops.rs:69-73): `P - x`, which wraps for non-canonical x.
+  HB_HD static W neg_ref(W a) { return a == 0 ? 0 : P - a; }
+  HB_HD static W value(W a) { return canon(a); }
+  // Plain (non-Montgomery) constant: identity for Goldilocks.
+  HB_HD static W to_mont(W a) { return a; }
+  // CT butterfly: (x, y) -> (x + w y, x - w y) with w canonical.
+  HB_HD static void ct(W &x, W &y, W w) {
+    const W t = mul(y, w);
+    const W u = x;
+    x = add_c(u, t);
+    y = sub_c(u, t);
+  }
+  // GS butterfly: (x, y) -> (x + y, (x - y) w).
+  HB_HD static void gs(W &x, W &y, W w) {
+    const W u = x, v = y;
+    x = add(u, v);
+    y = mul(sub(u, v), w);
+  }
+  // acc += x * k with k canonical-premultiplied key word.
+  HB_HD static W mac(W acc, W x, W k) { return add_c(acc, mul(x, k)); }
+};
+
+struct BabyBear {
+  using W = uint32_t;
+  static constexpr W P = 0x78000001U;
+  static constexpr W PINV_NEG = 0x77FFFFFFU;  // -P^-1 mod 2^32
+  static constexpr int BITS = 31;
+  static constexpr int FIELD_ID = 0;
+
+  HB_HD static W canon(W x) { return x >= P ? x - P : x; }
+  // Montgomery product a*b*2^-32 mod P for a*b < P*2^32; canonical result.
+  HB_HD static W mont(W a, W b) {
+    const uint64_t t = (uint64_t)a * b;
+    const uint32_t m = (uint32_t)t * PINV_NEG;
+    const uint64_t u = (t + (uint64_t)m * P) >> 32;
+    const uint32_t r = (uint32_t)u;
+    return r >= P ? r - P : r;
+  }
+  HB_HD static W mul(W a, W b_mont) { return mont(a, b_mont); }
+  HB_HD static W add(W a, W b) {
+    const W s = a + b;
+    return s >= P ? s - P : s;
+  }
+  HB_HD static W sub(W a, W b) { return a >= b ? a - b : a + P - b; }
+  HB_HD static W add_c(W a, W b) { return add(a, b); }
+  HB_HD static W sub_c(W a, W b) { return sub(a, b); }
+  HB_HD static W neg_ref(W a) { return a == 0 ? 0 : P - a; }
+  HB_HD static W value(W a) { return a; }
+  HB_HD static W to_mont(W a) { return (W)(((uint64_t)a << 32) % P); }
+  HB_HD static void ct(W &x, W &y, W w) {
+    const W t = mont(y, w);
+    const W u = x;
+    x = add(u, t);
+    y = sub(u, t);
+  }
+  HB_HD static void gs(W &x, W &y, W w) {
+    const W u = x, v = y;
+    x = add(u, v);
+    y = mont(sub(u, v), w);
+  }
+  HB_HD static W mac(W acc, W x, W k) { return add(acc, mont(x, k)); }
+};
+
+// Host-side exact helpers used to build tables.
+template <class F>
+inline typename F::W host_mulmod(typename F::W a, typename F::W b) {
+  return (typename F::W)(((unsigned __int128)a * b) % F::P);
+}
+template <class F>
+inline typename F::W host_powmod(typename F::W b, uint64_t e) {
+  typename F::W r = 1;
+  while (e) {
+    if (e & 1) r = host_mulmod<F>(r, b);
+    b = host_mulmod<F>(b, b);
+    e >>= 1;
+  }
+  return r;
+}
+
+}  // namespace hb

@@ -1,0 +1,553 @@
+// hb_kernels.cuh -- sm_100a kernels of the TFHE gate-bootstrapping path.
+//
+//  * prepare_polys_kernel   coefficient-domain key polynomials -> device NTT slot layout, scaled by
+//                           N^-1 (and R for BabyBear) so the inverse transform needs no normalising
+//  * ntt_roundtrip_kernel   batched forward + inverse negacyclic NTT (kernel microbench)
+//  * ntt_fwd/inv_kernel     AbstractNTT::{transform_slice, inverse_transform_slice} on device slices
+//  * ext_product_kernel     RLWE x RGSW external product for many RLWEs sharing one RGSW
+//  * bootstrap_kernel       persistent batched gate bootstrapping: modulus switch, blind rotation
+//                           with accumulators in shared memory, key switching and sample extraction,
+//                           G gates per CTA sharing every bootstrapping-key chunk, which the TMA unit
+//                           streams into a ring of shared-memory stages
+#pragma once
+
+#include "hb_field.cuh"
+#include "hb_ntt.cuh"
+#include "hb_sync.cuh"
+
+namespace hb {
+
+enum : int { STATUS_OK = 0, STATUS_TIMEOUT = 1 };
+
+// ------------------------------------------------------------------------------------------
+// Shared pieces
+// ------------------------------------------------------------------------------------------
+
+// lwe_modulus_switch (fhe_core/src/modulus_switch.rs:12-38): round(f64(v) * 2N / f64(Q)) mod 2N
+// with IEEE round-to-nearest conversion, multiply and divide, and round-half-away-from-zero.
+template <class F>
+__device__ __forceinline__ uint32_t modswitch(typename F::W v, uint32_t two_n) {
+  const double x = __ull2double_rn((unsigned long long)F::value(v));
+  const double q = __ull2double_rn((unsigned long long)F::P);
+  const double r = round(__ddiv_rn(__dmul_rn(x, (double)two_n), q));
+  const uint32_t t = (uint32_t)(unsigned long long)r;
+  return t < two_n ? t : t - two_n;
+}
+
+template <class F>
+__device__ __forceinline__ typename F::W canon_neg(typename F::W x) {
+  x = F::canon(x);
+  return x == 0 ? 0 : F::P - x;
+}
+
+// s * x for s in {-2,...,2}, canonical result.
+template <class F>
+__device__ __forceinline__ typename F::W small_mul(typename F::W x, int s) {
+  using W = typename F::W;
+  x = F::canon(x);
+  W y = s == 2 || s == -2 ? F::canon(F::add(x, x)) : (s == 0 ? 0 : x);
+  return s < 0 ? canon_neg<F>(y) : y;
+}
+
+// One gate job: `count` gates whose input LWE ciphertexts are combined as
+// c = s0*c0 + s1*c1 + s2*c2 (+ add_b on the body), then bootstrapped with a LUT that is either a
+// caller polynomial (`lut`) or the piecewise constant {lo on [0, mid), hi on [mid, N)} of the gate
+// LUT builders (tfhe/src/bfhe/evaluate.rs:267-465).
+struct GateJob {
+  const void *in0, *in1, *in2;
+  void *out;
+  const void *lut;
+  unsigned long long lut_lo, lut_hi, add_b;
+  uint32_t lut_mid;
+  int32_t s0, s1, s2;
+  uint32_t count;
+  uint32_t first_batch;
+};
+
+// Ring of S shared-memory stages fed by the TMA unit with consecutive 2N-word chunks of key
+// material; all G groups of the CTA consume chunk c from stage c % S, then the CTA releases it and
+// one thread refills it with chunk c + S.
+template <class W, int N, int S>
+struct ChunkPipe {
+  W *stages;
+  uint64_t *bars;
+  volatile int *abort_flag;
+  int *status;
+  long long budget;
+  unsigned long long next;   // next chunk to consume
+  unsigned long long total;  // chunks this CTA consumes in the whole launch
+  static constexpr uint32_t WORDS = 2 * N;
+  static constexpr uint32_t BYTES = WORDS * sizeof(W);
+
+  template <class Src>
+  __device__ __forceinline__ void prime(const Src &src) {
+    if (threadIdx.x == 0)
+      for (unsigned long long c = 0; c < (unsigned long long)S && c < total; ++c) {
+        mbar_arrive_expect_tx(&bars[c], BYTES);
+        bulk_g2s(stages + c * WORDS, src(c), BYTES, &bars[c]);
+      }
+  }
+  // Wait until the current chunk has landed; returns its stage.
+  __device__ __forceinline__ const W *acquire() {
+    const int st = (int)(next % S);
+    const uint32_t par = (uint32_t)((next / S) & 1);
+    if (!mbar_wait_bounded(&bars[st], par, budget)) {
+      *abort_flag = 1;
+      atomicOr(status, STATUS_TIMEOUT);
+    }
+    return stages + st * WORDS;
+  }
+  // CTA-wide release of the current chunk and refill; false when the launch must stop.
+  template <class Src>
+  __device__ __forceinline__ bool release(const Src &src) {
+    __syncthreads();
+    if (*abort_flag) {
+      drain();
+      return false;
+    }
+    if (threadIdx.x == 0 && next + S < total) {
+      const int st = (int)(next % S);
+      mbar_arrive_expect_tx(&bars[st], BYTES);
+      bulk_g2s(stages + st * WORDS, src(next + S), BYTES, &bars[st]);
+    }
+    ++next;
+    return true;
+  }
+  // On abort: wait (bounded) for the copies this CTA still has in flight before leaving.
+  __device__ __forceinline__ void drain() {
+    if (threadIdx.x != 0) return;
+    for (unsigned long long c = next; c < next + S && c < total; ++c)
+      mbar_wait_bounded(&bars[c % S], (uint32_t)((c / S) & 1), budget);
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// Key preparation
+// ------------------------------------------------------------------------------------------
+
+// in: npolys coefficient-domain polynomials (natural order, canonical); out: same count in the
+// device slot layout out[poly][v*T + t] = scale * NTT(in)[slot t*V + v].
+template <class F, int LOGN, int T>
+__global__ void __launch_bounds__(2 * T) prepare_polys_kernel(const typename F::W *__restrict__ in,
+                                                             typename F::W *__restrict__ out,
+                                                             unsigned long long npolys,
+                                                             const typename F::W *__restrict__ tw_g,
+                                                             typename F::W scale) {
+  using W = typename F::W;
+  using NT = GroupNtt<F, LOGN, T>;
+  constexpr int N = 1 << LOGN, V = NT::V;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  W *s_tw = reinterpret_cast<W *>(smem_raw);
+  W *s_x = s_tw + N;
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s_tw[i] = tw_g[i];
+  __syncthreads();
+  GroupSync<T> sync{1 + g};
+  W *xbuf = s_x + g * 2 * N;
+  int ping = 0;
+  for (unsigned long long poly = (unsigned long long)blockIdx.x * 2 + g; poly < npolys;
+       poly += (unsigned long long)gridDim.x * 2) {
+    W x[V];
+    const W *src = in + poly * N;
+#pragma unroll
+    for (int v = 0; v < V; ++v) x[v] = F::canon(src[NT::natural_pos(t, v)]);
+    NT::forward(x, xbuf, ping, s_tw, t, sync);
+    W *dst = out + poly * N;
+#pragma unroll
+    for (int v = 0; v < V; ++v) dst[v * T + t] = F::mul(x[v], scale);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Batched NTT kernels (one polynomial per thread group)
+// ------------------------------------------------------------------------------------------
+
+// mode 0: forward then inverse with N^-1 (round trip), 1: forward only (slot order out),
+// 2: inverse only (slot order in, N^-1 applied).
+template <class F, int LOGN, int T, int GPB>
+__global__ void __launch_bounds__(GPB * T) ntt_batch_kernel(const typename F::W *in,  // may alias out
+                                                           typename F::W *out,
+                                                           unsigned long long npolys,
+                                                           const typename F::W *__restrict__ tw_g,
+                                                           const typename F::W *__restrict__ itw_g,
+                                                           typename F::W n_inv, int mode) {
+  using W = typename F::W;
+  using NT = GroupNtt<F, LOGN, T>;
+  constexpr int N = 1 << LOGN, V = NT::V;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  W *s_tw = reinterpret_cast<W *>(smem_raw);
+  W *s_itw = s_tw + N;
+  W *s_x = s_itw + N;
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    s_tw[i] = tw_g[i];
+    s_itw[i] = itw_g[i];
+  }
+  __syncthreads();
+  GroupSync<T> sync{1 + g};
+  W *xbuf = s_x + g * 2 * N;
+  int ping = 0;
+  for (unsigned long long poly = (unsigned long long)blockIdx.x * GPB + g; poly < npolys;
+       poly += (unsigned long long)gridDim.x * GPB) {
+    W x[V];
+    const W *src = in + poly * N;
+    W *dst = out + poly * N;
+    if (mode == 2) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) x[v] = src[NT::slot_pos(t, v)];
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) x[v] = src[NT::natural_pos(t, v)];
+    }
+    if (mode != 2) NT::forward(x, xbuf, ping, s_tw, t, sync);
+    if (mode == 1) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) dst[NT::slot_pos(t, v)] = F::canon(x[v]);
+      continue;
+    }
+    NT::inverse(x, xbuf, ping, s_itw, t, sync);
+#pragma unroll
+    for (int v = 0; v < V; ++v) dst[NT::natural_pos(t, v)] = F::mul(x[v], n_inv);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// External product: out_i = RLWE_i x RGSW (lattice/src/rlwe.rs:573-596) for many RLWEs
+// ------------------------------------------------------------------------------------------
+
+template <class F, int LOGN, int T, int G, int S>
+__global__ void __launch_bounds__(G * T, 1)
+    ext_product_kernel(const typename F::W *__restrict__ rlwe_in, typename F::W *__restrict__ rlwe_out,
+                       unsigned long long count, const typename F::W *__restrict__ rgsw,
+                       uint32_t len, uint32_t bits, const typename F::W *__restrict__ tw_g,
+                       const typename F::W *__restrict__ itw_g, int *status, long long budget) {
+  using W = typename F::W;
+  using NT = GroupNtt<F, LOGN, T>;
+  constexpr int N = 1 << LOGN, V = NT::V;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  W *s_tw = reinterpret_cast<W *>(smem_raw);
+  W *s_itw = s_tw + N;
+  W *s_k = s_itw + N;
+  W *s_x = s_k + S * 2 * N;
+  uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_x + G * 2 * N);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_bar + S);
+  const int tid = threadIdx.x, g = tid / T, t = tid % T;
+  for (int i = tid; i < N; i += blockDim.x) {
+    s_tw[i] = tw_g[i];
+    s_itw[i] = itw_g[i];
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&s_bar[s], 1);
+    mbar_fence_init();
+    *s_abort = 0;
+  }
+  __syncthreads();
+  GroupSync<T> sync{1 + g};
+  W *xbuf = s_x + g * 2 * N;
+  int ping = 0;
+
+  const unsigned long long batches = (count + G - 1) / G;
+  const unsigned long long my_batches =
+      blockIdx.x < batches ? (batches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t cpb = 2 * len;
+  ChunkPipe<W, N, S> pipe{s_k, s_bar, s_abort, status, budget, 0, my_batches * cpb};
+  auto src = [&](unsigned long long c) { return rgsw + (size_t)(c % cpb) * 2 * N; };
+  pipe.prime(src);
+  const uint64_t mask = (bits >= 64) ? ~0ULL : ((1ULL << bits) - 1);
+
+  for (unsigned long long b = blockIdx.x; b < batches; b += gridDim.x) {
+    const unsigned long long item = b * G + g;
+    const bool active = item < count;
+    W acc_a[V], acc_b[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc_a[v] = acc_b[v] = 0;
+    for (int part = 0; part < 2; ++part) {
+      W e[V];
+      if (active) {
+        const W *src_poly = rlwe_in + (item * 2 + part) * N;
+#pragma unroll
+        for (int v = 0; v < V; ++v) e[v] = F::value(src_poly[NT::natural_pos(t, v)]);
+      }
+      for (uint32_t j = 0; j < len; ++j) {
+        W x[V];
+        if (active) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> (j * bits)) & mask);
+          NT::forward(x, xbuf, ping, s_tw, t, sync);
+        }
+        const W *k = pipe.acquire();
+        if (active) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            acc_a[v] = F::mac(acc_a[v], x[v], k[v * T + t]);
+            acc_b[v] = F::mac(acc_b[v], x[v], k[N + v * T + t]);
+          }
+        }
+        if (!pipe.release(src)) return;
+      }
+    }
+    if (active) {
+      NT::inverse(acc_a, xbuf, ping, s_itw, t, sync);
+      NT::inverse(acc_b, xbuf, ping, s_itw, t, sync);
+      W *dst = rlwe_out + item * 2 * N;
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        dst[NT::natural_pos(t, v)] = F::canon(acc_a[v]);
+        dst[N + NT::natural_pos(t, v)] = F::canon(acc_b[v]);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Persistent batched bootstrapping (EvaluationKey::bootstrap, tfhe/src/bfhe/evaluate.rs:42-60)
+// ------------------------------------------------------------------------------------------
+
+template <class W>
+struct BootParams {
+  const W *bsk;  // [n][2][len][2][N] slot layout, scaled (one 2N-word chunk per (i, part, j))
+  const W *ksk;  // [ks_len][2][N] slot layout, scaled
+  const W *tw, *itw;
+  const GateJob *jobs;
+  int njobs;
+  uint32_t total_batches;
+  uint32_t n, len, bits, ks_len, ks_bits;
+  int *status;
+  long long budget;
+};
+
+// Shared memory words needed by bootstrap_kernel.
+template <class W, int N, int G, int S>
+__host__ __device__ constexpr size_t boot_smem_bytes(uint32_t n) {
+  return sizeof(W) * (size_t)(2 * N + S * 2 * N + G * 4 * N) + sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) +
+         sizeof(uint64_t) * S + 16;
+}
+
+template <class F, int LOGN, int T, int G, int S>
+__global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<typename F::W> p) {
+  using W = typename F::W;
+  using NT = GroupNtt<F, LOGN, T>;
+  constexpr int N = 1 << LOGN, V = NT::V;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  W *s_tw = reinterpret_cast<W *>(smem_raw);
+  W *s_itw = s_tw + N;
+  W *s_k = s_itw + N;
+  W *s_grp = s_k + S * 2 * N;
+  const uint32_t msz = (p.n + 8) & ~7u;
+  uint16_t *s_ms = reinterpret_cast<uint16_t *>(s_grp + G * 4 * N);
+  uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_ms + G * msz);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_bar + S);
+
+  const int tid = threadIdx.x, g = tid / T, t = tid % T;
+  for (int i = tid; i < N; i += blockDim.x) {
+    s_tw[i] = p.tw[i];
+    s_itw[i] = p.itw[i];
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&s_bar[s], 1);
+    mbar_fence_init();
+    *s_abort = 0;
+  }
+  __syncthreads();
+
+  GroupSync<T> sync{1 + g};
+  W *acc_a = s_grp + g * 4 * N;
+  W *acc_b = acc_a + N;
+  W *xbuf = acc_b + N;
+  uint16_t *ms = s_ms + g * msz;
+  int ping = 0;
+
+  const uint32_t n = p.n;
+  const uint32_t br_chunks = n * 2 * p.len;
+  const uint32_t cpb = br_chunks + p.ks_len;
+  const uint32_t my_batches =
+      blockIdx.x < p.total_batches ? (p.total_batches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  ChunkPipe<W, N, S> pipe{s_k, s_bar, s_abort, p.status, p.budget, 0,
+                          (unsigned long long)my_batches * cpb};
+  auto src = [&](unsigned long long c) -> const W * {
+    const uint32_t q = (uint32_t)(c % cpb);
+    return q < br_chunks ? p.bsk + (size_t)q * 2 * N : p.ksk + (size_t)(q - br_chunks) * 2 * N;
+  };
+  pipe.prime(src);
+
+  const uint64_t br_mask = (1ULL << p.bits) - 1;
+  const uint64_t ks_mask = (1ULL << p.ks_bits) - 1;
+  const uint32_t two_n = 2 * N;
+
+  for (uint32_t batch = blockIdx.x; batch < p.total_batches; batch += gridDim.x) {
+    int jx = 0;
+    while (jx + 1 < p.njobs && p.jobs[jx + 1].first_batch <= batch) ++jx;
+    const GateJob &job = p.jobs[jx];
+    const uint32_t gate = (batch - job.first_batch) * G + g;
+    const bool active = gate < job.count;
+    const size_t lwe_words = (size_t)n + 1;
+
+    // ---- input combine + modulus switch (Evaluator::nand etc., evaluate.rs:113-119) ----
+    if (active) {
+      const W *c0 = reinterpret_cast<const W *>(job.in0) + gate * lwe_words;
+      const W *c1 = job.in1 ? reinterpret_cast<const W *>(job.in1) + gate * lwe_words : nullptr;
+      const W *c2 = job.in2 ? reinterpret_cast<const W *>(job.in2) + gate * lwe_words : nullptr;
+      for (uint32_t k = t; k <= n; k += T) {
+        W c = small_mul<F>(c0[k], job.s0);
+        if (c1) c = F::canon(F::add(c, small_mul<F>(c1[k], job.s1)));
+        if (c2) c = F::canon(F::add(c, small_mul<F>(c2[k], job.s2)));
+        if (k == n) c = F::canon(F::add(c, (W)job.add_b));
+        ms[k] = (uint16_t)modswitch<F>(c, two_n);
+      }
+    }
+    sync();
+    // ---- ACC = (0, LUT * X^{-b}) (fhe_core/src/blind_rotation/rlwe/binary.rs:40-64) ----
+    if (active) {
+      const uint32_t bt = ms[n];
+      const int e = bt ? (int)(two_n - bt) : 0;
+      const W *lut = reinterpret_cast<const W *>(job.lut);
+      for (int k = t; k < N; k += T) {
+        int s = k - e;
+        bool neg = false;
+        if (s < 0) {
+          s += N;
+          neg = true;
+          if (s < 0) {
+            s += N;
+            neg = false;
+          }
+        }
+        W f = lut ? F::canon(lut[s]) : (W)((uint32_t)s < job.lut_mid ? job.lut_lo : job.lut_hi);
+        acc_a[k] = 0;
+        acc_b[k] = neg ? F::neg_ref(f) : f;
+      }
+    }
+    sync();
+
+    // ---- blind rotation (binary.rs:66-103) ----
+    W acc_x[V], acc_y[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc_x[v] = acc_y[v] = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      const int r = active ? (int)ms[i] : 0;
+      for (int part = 0; part < 2; ++part) {
+        // E = ACC * (X^r - 1) (lattice/src/rlwe.rs:437-487) in the reference's representation,
+        // then canonical for the unsigned decomposition.
+        W e[V];
+        if (active) {
+          const W *y = part == 0 ? acc_a : acc_b;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const int k = NT::natural_pos(t, v);
+            int s = k - r;
+            W rot;
+            if (s >= 0) {
+              rot = y[s];
+            } else if (s >= -N) {
+              rot = F::neg_ref(y[s + N]);
+            } else {
+              rot = y[s + 2 * N];
+            }
+            e[v] = F::value(F::sub(rot, y[k]));
+          }
+        }
+        for (uint32_t j = 0; j < p.len; ++j) {
+          W x[V];
+          if (active) {
+            const uint32_t sh = j * p.bits;
+#pragma unroll
+            for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & br_mask);
+            NT::forward(x, xbuf, ping, s_tw, t, sync);
+          }
+          const W *k = pipe.acquire();
+          if (active) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              acc_x[v] = F::mac(acc_x[v], x[v], k[v * T + t]);
+              acc_y[v] = F::mac(acc_y[v], x[v], k[N + v * T + t]);
+            }
+          }
+          if (!pipe.release(src)) return;
+        }
+      }
+      if (active) {
+        NT::inverse(acc_x, xbuf, ping, s_itw, t, sync);
+        NT::inverse(acc_y, xbuf, ping, s_itw, t, sync);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const int k = NT::natural_pos(t, v);
+          acc_a[k] = F::add(acc_a[k], F::canon(acc_x[v]));  // RLWE::add_assign_element_wise
+          acc_b[k] = F::add(acc_b[k], F::canon(acc_y[v]));
+          acc_x[v] = acc_y[v] = 0;
+        }
+      }
+      sync();
+    }
+
+    // ---- key switching + sample extraction (fhe_core/src/key_switch/rlwe.rs:115-137,250-286) ----
+    {
+      W e[V];
+      if (active) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) e[v] = F::value(F::neg_ref(acc_a[NT::natural_pos(t, v)]));
+      }
+      for (uint32_t j = 0; j < p.ks_len; ++j) {
+        W x[V];
+        if (active) {
+          const uint32_t sh = j * p.ks_bits;
+#pragma unroll
+          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & ks_mask);
+          NT::forward(x, xbuf, ping, s_tw, t, sync);
+        }
+        const W *k = pipe.acquire();
+        if (active) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            acc_x[v] = F::mac(acc_x[v], x[v], k[v * T + t]);
+            acc_y[v] = F::mac(acc_y[v], x[v], k[N + v * T + t]);
+          }
+        }
+        if (!pipe.release(src)) return;
+      }
+      if (active) {
+        NT::inverse(acc_x, xbuf, ping, s_itw, t, sync);
+        NT::inverse(acc_y, xbuf, ping, s_itw, t, sync);
+        // acc.b[0] += Q >> 3 (evaluate.rs:52), then b' = b0 + INTT(...)[0]
+        const W b0 = F::canon(F::add(acc_b[0], (W)(F::P >> 3)));
+        W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const int k = NT::natural_pos(t, v);
+          const W a_k = F::canon(acc_x[v]);
+          if (k == 0) {
+            out[0] = a_k;
+            out[n] = F::canon(F::add(F::canon(acc_y[v]), b0));
+          } else if (k >= N - (int)n + 1) {
+            out[N - k] = F::neg_ref(a_k);  // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402)
+          }
+          acc_x[v] = acc_y[v] = 0;
+        }
+      }
+      sync();
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Integer-pipe modmul throughput probe (roofline denominator): every thread runs 8 independent
+// chains of F::mul on register operands; the result is stored so nothing is dead code.
+// ------------------------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(256) modmul_probe_kernel(typename F::W *out, uint32_t iters,
+                                                            typename F::W seed) {
+  using W = typename F::W;
+  W x[8];
+  const W w = (W)(seed | 3u);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x[i] = F::canon((W)(seed + threadIdx.x * 8u + i + blockIdx.x * 977u));
+  for (uint32_t it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = F::mul(x[i], w);
+  }
+  W acc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc ^= x[i];
+  out[blockIdx.x * (size_t)blockDim.x + threadIdx.x] = acc;
+}
+
+}  // namespace hb

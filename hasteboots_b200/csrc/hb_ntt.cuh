@@ -1,0 +1,161 @@
+// hb_ntt.cuh -- negacyclic NTT/INTT of one polynomial by a group of T threads, V = N/T words per
+// thread held in registers, exchanges through a swizzled shared-memory buffer between passes.
+//
+// Forward: Cooley-Tukey with merged psi powers (natural order in, bit-reversed slot order out).
+// Inverse: Gentleman-Sande (bit-reversed slot order in, natural order out), without the final
+// N^-1 scaling (callers fold N^-1 into the key material they multiply by, or scale explicitly).
+// This replaces concrete-ntt's Plan::fwd / Plan::inv + normalize behind
+// AbstractNTT::{transform_slice, inverse_transform_slice} (algebra/src/transformation/concrete.rs:116-148).
+//
+// Register layout of a pass with "low" position `lo`: thread t, register v holds element
+//   idx(t, v, lo) = ((t >> lo) << (lo + LOGV)) | (v << lo) | (t & ((1 << lo) - 1)).
+// Forward passes cover butterfly bits from the top down (LOGV bits per pass); the last forward
+// pass and the first inverse pass share layout lo = 0 (thread t holds slots t*V .. t*V+V-1), so the
+// pointwise multiply-accumulate between them needs no exchange.
+#pragma once
+
+#include "hb_field.cuh"
+
+namespace hb {
+
+__host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x >> 1); }
+
+// Synchronisation of one thread group: a warp (T == 32) or a named barrier (T > 32).
+template <int T>
+struct GroupSync {
+  int bar_id;
+  __device__ __forceinline__ void operator()() const {
+    if constexpr (T == 32) {
+      __syncwarp();
+    } else {
+      asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(T) : "memory");
+    }
+  }
+};
+
+template <class F, int LOGN, int T>
+struct GroupNtt {
+  using W = typename F::W;
+  static constexpr int N = 1 << LOGN;
+  static constexpr int V = N / T;
+  static constexpr int LOGV = ilog2c(V);
+  static constexpr int LOGT = LOGN - LOGV;
+  static constexpr int SWZ = sizeof(W) == 8 ? 15 : 31;
+  static_assert((1 << LOGV) == V && V >= 2, "V must be a power of two >= 2");
+  static_assert(T % 32 == 0, "groups are whole warps");
+
+  // Physical slot of element q in an exchange buffer: an XOR swizzle that makes every pass layout
+  // conflict-free (half-warp distinct banks for 8-byte words, warp-distinct for 4-byte words).
+  __device__ __forceinline__ static int phys(int q) { return q ^ ((q >> LOGV) & SWZ); }
+
+  template <int LO>
+  __device__ __forceinline__ static int idx(int t, int v) {
+    return ((t >> LO) << (LO + LOGV)) | (v << LO) | (t & ((1 << LO) - 1));
+  }
+
+  // Natural-order position held by (t, v) at the forward input / inverse output layout.
+  __device__ __forceinline__ static int natural_pos(int t, int v) { return v * T + t; }
+  // Slot held by (t, v) at the forward output / inverse input layout.
+  __device__ __forceinline__ static int slot_pos(int t, int v) { return t * V + v; }
+
+  template <int LO_FROM, int LO_TO>
+  __device__ __forceinline__ static void exchange(W (&x)[V], W *buf, int t, const GroupSync<T> &sync) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) buf[phys(idx<LO_FROM>(t, v))] = x[v];
+    sync();
+#pragma unroll
+    for (int v = 0; v < V; ++v) x[v] = buf[phys(idx<LO_TO>(t, v))];
+  }
+
+  // One forward (CT) stage on butterfly bit BB in a pass of layout LO.
+  template <int LO, int BB>
+  __device__ __forceinline__ static void fwd_stage(W (&x)[V], const W *__restrict__ tw, int t) {
+    constexpr int RB = BB - LO;
+    constexpr int S = LOGN - 1 - BB;
+    constexpr int K = V >> (RB + 1);  // distinct twiddles per thread in this stage
+    const int base = (1 << S) + ((t >> LO) << (LOGV - RB - 1));
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const W w = tw[base + k];
+#pragma unroll
+      for (int l = 0; l < (1 << RB); ++l) {
+        const int v = (k << (RB + 1)) | l;
+        F::ct(x[v], x[v | (1 << RB)], w);
+      }
+    }
+  }
+
+  template <int LO, int BB>
+  __device__ __forceinline__ static void inv_stage(W (&x)[V], const W *__restrict__ itw, int t) {
+    constexpr int RB = BB - LO;
+    constexpr int H = N >> (BB + 1);
+    constexpr int K = V >> (RB + 1);
+    const int base = H + ((t >> LO) << (LOGV - RB - 1));
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const W w = itw[base + k];
+#pragma unroll
+      for (int l = 0; l < (1 << RB); ++l) {
+        const int v = (k << (RB + 1)) | l;
+        F::gs(x[v], x[v | (1 << RB)], w);
+      }
+    }
+  }
+
+  // Forward pass whose top butterfly bit is TOP-1; recurses to the next pass.
+  template <int TOP, int BB>
+  __device__ __forceinline__ static void fwd_stages(W (&x)[V], const W *tw, int t) {
+    constexpr int LO = TOP - LOGV > 0 ? TOP - LOGV : 0;
+    constexpr int LAST = TOP - LOGV > 0 ? TOP - LOGV : 0;
+    fwd_stage<LO, BB>(x, tw, t);
+    if constexpr (BB - 1 >= LAST) fwd_stages<TOP, BB - 1>(x, tw, t);
+  }
+  template <int TOP>
+  __device__ __forceinline__ static void fwd_pass(W (&x)[V], W *buf, int &ping, const W *tw, int t,
+                                                  const GroupSync<T> &sync) {
+    constexpr int LO = TOP - LOGV > 0 ? TOP - LOGV : 0;
+    fwd_stages<TOP, TOP - 1>(x, tw, t);
+    if constexpr (LO > 0) {
+      constexpr int NEXT = LO - LOGV > 0 ? LO - LOGV : 0;
+      exchange<LO, NEXT>(x, buf + ping * N, t, sync);
+      ping ^= 1;
+      fwd_pass<LO>(x, buf, ping, tw, t, sync);
+    }
+  }
+
+  // Inverse pass processing bits [B0, min(B0+LOGV, LOGN)) in layout LO = min(B0, LOGN-LOGV).
+  template <int B0, int BB>
+  __device__ __forceinline__ static void inv_stages(W (&x)[V], const W *itw, int t) {
+    constexpr int LO = B0 < LOGN - LOGV ? B0 : LOGN - LOGV;
+    constexpr int END = B0 + LOGV < LOGN ? B0 + LOGV : LOGN;
+    inv_stage<LO, BB>(x, itw, t);
+    if constexpr (BB + 1 < END) inv_stages<B0, BB + 1>(x, itw, t);
+  }
+  template <int B0>
+  __device__ __forceinline__ static void inv_pass(W (&x)[V], W *buf, int &ping, const W *itw, int t,
+                                                  const GroupSync<T> &sync) {
+    constexpr int LO = B0 < LOGN - LOGV ? B0 : LOGN - LOGV;
+    constexpr int END = B0 + LOGV < LOGN ? B0 + LOGV : LOGN;
+    inv_stages<B0, B0>(x, itw, t);
+    if constexpr (END < LOGN) {
+      constexpr int NLO = END < LOGN - LOGV ? END : LOGN - LOGV;
+      exchange<LO, NLO>(x, buf + ping * N, t, sync);
+      ping ^= 1;
+      inv_pass<END>(x, buf, ping, itw, t, sync);
+    }
+  }
+
+  // x: natural-order values at natural_pos(t, v) -> slots at slot_pos(t, v).
+  // buf: two exchange buffers of N words (ping-pong), private to the group.
+  __device__ __forceinline__ static void forward(W (&x)[V], W *buf, int &ping, const W *tw, int t,
+                                                 const GroupSync<T> &sync) {
+    fwd_pass<LOGN>(x, buf, ping, tw, t, sync);
+  }
+  // x: slots at slot_pos(t, v) -> N * (natural-order values) at natural_pos(t, v).
+  __device__ __forceinline__ static void inverse(W (&x)[V], W *buf, int &ping, const W *itw, int t,
+                                                 const GroupSync<T> &sync) {
+    inv_pass<0>(x, buf, ping, itw, t, sync);
+  }
+};
+
+}  // namespace hb

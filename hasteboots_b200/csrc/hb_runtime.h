@@ -1,0 +1,58 @@
+// hb_runtime.h -- host-side context and key handles shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/hb_gpu.h"
+
+namespace hbrt {
+
+struct DevTables {
+  void *tw = nullptr;   // psi^brv(k) (Montgomery form for BabyBear)
+  void *itw = nullptr;  // psi^-brv(k)
+  unsigned long long n_inv = 0;      // multiplier giving x * N^-1
+  unsigned long long key_scale = 0;  // multiplier applied to key words at upload
+};
+
+struct Scratch {
+  void *ptr = nullptr;
+  size_t cap = 0;
+};
+
+}  // namespace hbrt
+
+struct hb_ctx {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  int *d_status = nullptr;
+  size_t budget = 0;
+  size_t in_use = 0;
+  std::vector<std::pair<void *, size_t>> sizes;
+  std::string err;
+  hbrt::DevTables tables[2][13];
+  hbrt::Scratch jobs, io, mux_tmp;
+  unsigned long long launches = 0;  // bootstrap kernel launches issued by this context
+};
+
+struct hb_keys {
+  hb_params p{};
+  void *bsk = nullptr;
+  void *ksk = nullptr;
+  size_t bytes = 0;
+};
+
+namespace hbrt {
+int fail(hb_ctx *ctx, int code, const char *fmt, ...);
+int cuda_fail(hb_ctx *ctx, cudaError_t e, const char *what);
+int dev_alloc(hb_ctx *ctx, size_t bytes, void **out);
+void dev_free(hb_ctx *ctx, void *p);
+int scratch(hb_ctx *ctx, Scratch &s, size_t bytes);
+int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out);
+int check_status(hb_ctx *ctx);
+long long wait_budget();
+}  // namespace hbrt

@@ -1,0 +1,276 @@
+"""Host-side mirror of the reference tfhe crate API over the C ABI of libhb_gpu.so.
+
+Names follow the reference (tfhe/src/lib.rs:1-13): parameter statics, KeyGen, SecretKeyPack,
+Encryptor, Decryptor, Evaluator with nand/and/or/nor/xor/xnor/majority/not/mux/bootstrap
+(tfhe/src/bfhe/evaluate.rs:65-262). Ciphertexts are numpy arrays (host) or torch CUDA tensors
+(device), shape [count, n + 1], dtype uint64 (Goldilocks) / uint32 (BabyBear), canonical values.
+Host arrays go through hb_gate (copies in and out included); device tensors through hb_gate_device
+on the context stream.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import HbParams, check, lib
+
+GATE_IDS = {"nand": 0, "and": 1, "or": 2, "nor": 3, "xor": 4, "xnor": 5, "majority": 6,
+            "not": 7, "mux": 8}
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(ctypes.c_void_p)
+    return ctypes.c_void_p(a.data_ptr())  # torch tensor
+
+
+class Parameters:
+    """fhe_core::Parameters for the binary-LWE-key RLWE bootstrapping sets."""
+
+    def __init__(self, raw: HbParams, name=""):
+        check(lib().hb_params_validate(ctypes.byref(raw)), "Parameters::new")
+        self.raw = raw
+        self.name = name
+
+    @classmethod
+    def preset(cls, pid):
+        raw = HbParams()
+        check(lib().hb_params_preset(pid, ctypes.byref(raw)), "hb_params_preset")
+        names = {0: "BABYBEAR_BINARY_128_BITS_PARAMETERS",
+                 1: "GOLDILOCKS_BINARY_128_BITS_PARAMETERS", 2: "ZAMA_BINARY_128_BITS_PARAMETERS"}
+        return cls(raw, names[pid])
+
+    @property
+    def field_id(self):
+        return self.raw.field_id
+
+    @property
+    def dtype(self):
+        return np.uint64 if self.raw.field_id == _lib.FIELD_GOLDILOCKS else np.uint32
+
+    @property
+    def modulus(self):
+        return 0xFFFFFFFF00000001 if self.raw.field_id == _lib.FIELD_GOLDILOCKS else 0x78000001
+
+    def lwe_dimension(self):
+        return self.raw.lwe_dim
+
+    def ring_dimension(self):
+        return self.raw.ring_dim
+
+    def sizes(self):
+        out = [ctypes.c_size_t() for _ in range(5)]
+        check(lib().hb_params_sizes(ctypes.byref(self.raw), *[ctypes.byref(o) for o in out]),
+              "hb_params_sizes")
+        keys = ("lwe_sk", "ring_sk", "bsk", "ksk", "lwe")
+        return {k: o.value for k, o in zip(keys, out)}
+
+
+def BABYBEAR_BINARY_128_BITS_PARAMETERS():
+    return Parameters.preset(0)
+
+
+def GOLDILOCKS_BINARY_128_BITS_PARAMETERS():
+    return Parameters.preset(1)
+
+
+def ZAMA_BINARY_128_BITS_PARAMETERS():
+    return Parameters.preset(2)
+
+
+class SecretKeyPack:
+    """fhe_core::SecretKeyPack (fhe_core/src/secret_key.rs:42-89), seeded."""
+
+    def __init__(self, params: Parameters, seed=0):
+        self.params = params
+        self.seed = seed
+        s = params.sizes()
+        self.lwe_secret_key = np.zeros(s["lwe_sk"], params.dtype)
+        self.ring_secret_key = np.zeros(s["ring_sk"], params.dtype)
+        check(lib().hb_keygen(ctypes.byref(params.raw), seed, _ptr(self.lwe_secret_key),
+                              _ptr(self.ring_secret_key), None, None, 0), "KeyGen")
+        self._next_index = 0
+
+    def evaluation_key_material(self, threads=0):
+        """BSK and KSK (coefficient domain) of this key pack (Evaluator::new's key generation)."""
+        s = self.params.sizes()
+        lwe = np.zeros(s["lwe_sk"], self.params.dtype)
+        ring = np.zeros(s["ring_sk"], self.params.dtype)
+        bsk = np.zeros(s["bsk"], self.params.dtype)
+        ksk = np.zeros(s["ksk"], self.params.dtype)
+        check(lib().hb_keygen(ctypes.byref(self.params.raw), self.seed, _ptr(lwe), _ptr(ring),
+                              _ptr(bsk), _ptr(ksk), threads), "KeyGen")
+        return bsk, ksk
+
+    def encrypt(self, bits, index0=None):
+        bits = np.ascontiguousarray(np.atleast_1d(bits), dtype=np.uint8)
+        if index0 is None:
+            index0 = self._next_index
+        self._next_index = index0 + len(bits)
+        out = np.zeros((len(bits), self.params.lwe_dimension() + 1), self.params.dtype)
+        check(lib().hb_encrypt(ctypes.byref(self.params.raw), _ptr(self.lwe_secret_key), self.seed,
+                               index0, _ptr(bits), len(bits), _ptr(out)), "encrypt")
+        return out
+
+    def decrypt_with_noise(self, cts):
+        cts = np.ascontiguousarray(cts, dtype=self.params.dtype).reshape(
+            -1, self.params.lwe_dimension() + 1)
+        bits = np.zeros(len(cts), np.uint8)
+        noise = np.zeros(len(cts), np.uint64)
+        check(lib().hb_decrypt(ctypes.byref(self.params.raw), _ptr(self.lwe_secret_key), _ptr(cts),
+                               len(cts), _ptr(bits), _ptr(noise)), "decrypt")
+        return bits, noise
+
+    def decrypt(self, cts):
+        return self.decrypt_with_noise(cts)[0]
+
+
+class KeyGen:
+    @staticmethod
+    def generate_secret_key(params: Parameters, seed=0):
+        return SecretKeyPack(params, seed)
+
+
+class Encryptor:
+    def __init__(self, sk: SecretKeyPack):
+        self.sk = sk
+
+    def encrypt(self, bits, index0=None):
+        return self.sk.encrypt(bits, index0)
+
+
+class Decryptor:
+    def __init__(self, sk: SecretKeyPack):
+        self.sk = sk
+
+    def decrypt(self, cts):
+        return self.sk.decrypt(cts)
+
+    def decrypt_with_noise(self, cts):
+        return self.sk.decrypt_with_noise(cts)
+
+
+class Context:
+    """One CUDA device + stream + HBM budget (hb_ctx)."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        h = ctypes.c_void_p()
+        check(lib().hb_ctx_create(device, hbm_budget, ctypes.byref(h)), "hb_ctx_create")
+        self.handle = h
+        self.device = device
+
+    def stream_ptr(self):
+        s = ctypes.c_void_p()
+        check(lib().hb_ctx_stream(self.handle, ctypes.byref(s)), "hb_ctx_stream", self.handle)
+        return s.value or 0
+
+    def synchronize(self):
+        check(lib().hb_ctx_synchronize(self.handle), "hb_ctx_synchronize", self.handle)
+
+    def hbm_in_use(self):
+        return lib().hb_ctx_hbm_in_use(self.handle)
+
+    def close(self):
+        if self.handle:
+            lib().hb_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceKeys:
+    """Device-resident BSK/KSK (hb_keys)."""
+
+    def __init__(self, ctx: Context, params: Parameters, bsk, ksk):
+        h = ctypes.c_void_p()
+        bsk = np.ascontiguousarray(bsk, params.dtype)
+        ksk = np.ascontiguousarray(ksk, params.dtype)
+        check(lib().hb_keys_upload(ctx.handle, ctypes.byref(params.raw), _ptr(bsk), _ptr(ksk),
+                                   ctypes.byref(h)), "hb_keys_upload", ctx.handle)
+        self.ctx = ctx
+        self.params = params
+        self.handle = h
+
+    def free(self):
+        if self.handle and self.ctx.handle:
+            lib().hb_keys_free(self.ctx.handle, self.handle)
+        self.handle = None
+
+
+class Evaluator:
+    """tfhe::Evaluator (tfhe/src/bfhe/evaluate.rs:65-262) on one B200."""
+
+    def __init__(self, sk: SecretKeyPack, ctx: Context = None, keys=None):
+        self.params = sk.params
+        self.ctx = ctx or Context()
+        if keys is None:
+            bsk, ksk = sk.evaluation_key_material()
+            keys = DeviceKeys(self.ctx, self.params, bsk, ksk)
+        self.keys = keys
+
+    def parameters(self):
+        return self.params
+
+    def _gate(self, name, c0, c1=None, c2=None):
+        gid = GATE_IDS[name]
+        w = self.params.lwe_dimension() + 1
+        if isinstance(c0, np.ndarray):
+            dt = self.params.dtype
+            c0 = np.ascontiguousarray(c0, dt).reshape(-1, w)
+            c1 = None if c1 is None else np.ascontiguousarray(c1, dt).reshape(-1, w)
+            c2 = None if c2 is None else np.ascontiguousarray(c2, dt).reshape(-1, w)
+            out = np.zeros_like(c0)
+            check(lib().hb_gate(self.ctx.handle, self.keys.handle, gid, _ptr(c0), _ptr(c1), _ptr(c2),
+                                _ptr(out), len(c0)), name, self.ctx.handle)
+            return out
+        import torch  # device tensors
+        out = torch.empty_like(c0)
+        torch.cuda.current_stream().synchronize()
+        check(lib().hb_gate_device(self.ctx.handle, self.keys.handle, gid, _ptr(c0), _ptr(c1),
+                                   _ptr(c2), _ptr(out), c0.shape[0]), name, self.ctx.handle)
+        self.ctx.synchronize()
+        return out
+
+    def nand(self, c0, c1):
+        return self._gate("nand", c0, c1)
+
+    def and_(self, c0, c1):
+        return self._gate("and", c0, c1)
+
+    def or_(self, c0, c1):
+        return self._gate("or", c0, c1)
+
+    def nor(self, c0, c1):
+        return self._gate("nor", c0, c1)
+
+    def xor(self, c0, c1):
+        return self._gate("xor", c0, c1)
+
+    def xnor(self, c0, c1):
+        return self._gate("xnor", c0, c1)
+
+    def majority(self, c0, c1, c2):
+        return self._gate("majority", c0, c1, c2)
+
+    def not_(self, c0):
+        return self._gate("not", c0)
+
+    def mux(self, c0, c1, c2):
+        return self._gate("mux", c0, c1, c2)
+
+    def bootstrap(self, c, lut):
+        dt = self.params.dtype
+        c = np.ascontiguousarray(c, dt).reshape(-1, self.params.lwe_dimension() + 1)
+        lut = np.ascontiguousarray(lut, dt)
+        out = np.zeros_like(c)
+        check(lib().hb_bootstrap_lut(self.ctx.handle, self.keys.handle, _ptr(c), _ptr(lut),
+                                     _ptr(out), len(c)), "bootstrap", self.ctx.handle)
+        return out

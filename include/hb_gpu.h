@@ -1,0 +1,181 @@
+/*
+ * hb_gpu.h -- C ABI of the B200 (sm_100a) TFHE gate-bootstrapping library (libhb_gpu.so).
+ *
+ * Drop-in boundary for HasteBoots' bootstrapping path: the tfhe crate's Evaluator / KeyGen /
+ * Encryptor / Decryptor (tfhe/src/lib.rs:1-13, tfhe/src/bfhe/evaluate.rs), the lattice crate's
+ * RLWE x RGSW external product (lattice/src/rlwe.rs:573-596) and the algebra crate's NTT-table trait
+ * (algebra/src/transformation/mod.rs:20-96). A Rust binding (hb-gpu-sys) declares these functions
+ * verbatim in an `extern "C"` block; see INTEGRATION.md.
+ *
+ * Conventions
+ *  - Every function returns an int status: HB_OK (0) or a negative HB_ERR_* code. After an error,
+ *    hb_last_error() on the same context returns a one-line description. The Rust shim maps
+ *    non-zero statuses to panics where the reference panics (tfhe/src/bfhe/evaluate.rs:56) and to
+ *    Err where it returns Result (Parameters::new, fhe_core/src/parameter.rs:111).
+ *  - Field words are canonical little-endian values: uint64_t for Goldilocks
+ *    (Q = 2^64 - 2^32 + 1), uint32_t for BabyBear (Q = 2^31 - 2^27 + 1).
+ *  - An LWE ciphertext is n+1 words: a[0..n) then b. Batches are contiguous arrays of them.
+ *  - Key material in host buffers is coefficient domain: BSK layout
+ *    [i < n][part: 0 = c_neg_s_m, 1 = c_m][j < br_len][0 = a, 1 = b][N], KSK layout
+ *    [j < ks_len][0 = a, 1 = b][N] (NTTRGSW lattice/src/rgsw.rs:212-218, NTTGadgetRLWE
+ *    lattice/src/gadget/rlwe.rs:235-240, KeySwitchingRLWEKey fhe_core/src/key_switch/rlwe.rs:23-28).
+ *  - Functions named *_device take device pointers and enqueue on the context's stream without
+ *    synchronising; all other functions take host pointers and return when results are in place.
+ *  - A context is used by one host thread at a time.
+ */
+#ifndef HB_GPU_H
+#define HB_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HB_OK 0
+#define HB_ERR_INVALID (-1)     /* bad argument or parameter set */
+#define HB_ERR_CUDA (-2)        /* CUDA runtime error */
+#define HB_ERR_NOMEM (-3)       /* allocation would exceed the context's HBM budget */
+#define HB_ERR_TIMEOUT (-4)     /* a kernel's bounded wait ran out; results are invalid */
+#define HB_ERR_UNSUPPORTED (-5) /* parameter combination without a compiled kernel */
+#define HB_ERR_BUSY (-6)        /* serving queue full */
+
+#define HB_FIELD_BABYBEAR 0
+#define HB_FIELD_GOLDILOCKS 1
+
+/* Parameter-set ids (tfhe/src/bfhe/parameters.rs:45-117). */
+#define HB_PRESET_BABYBEAR_BINARY_128_BITS 0
+#define HB_PRESET_GOLDILOCKS_BINARY_128_BITS 1
+#define HB_PRESET_ZAMA_BINARY_128_BITS 2
+
+/* Gate ids (Evaluator::{nand, and, or, nor, xor, xnor, majority, not, mux},
+ * tfhe/src/bfhe/evaluate.rs:98-262). */
+#define HB_GATE_NAND 0
+#define HB_GATE_AND 1
+#define HB_GATE_OR 2
+#define HB_GATE_NOR 3
+#define HB_GATE_XOR 4
+#define HB_GATE_XNOR 5
+#define HB_GATE_MAJORITY 6
+#define HB_GATE_NOT 7
+#define HB_GATE_MUX 8
+
+typedef struct hb_ctx hb_ctx;
+typedef struct hb_keys hb_keys;
+
+/* fhe_core::ConstParameters (fhe_core/src/parameter.rs:81-107), binary LWE key branch. */
+typedef struct hb_params {
+  int32_t field_id;      /* HB_FIELD_* */
+  uint32_t ring_dim;     /* N (1024 is compiled) */
+  uint32_t lwe_dim;      /* n, with next_pow2(n) == N */
+  uint32_t br_bits;      /* blind_rotation_basis_bits */
+  uint32_t br_len;       /* ceil(bits(Q) / br_bits) (Basis::new, algebra/src/decompose_basis.rs:29-40) */
+  uint32_t ks_bits;      /* key_switching_basis_bits */
+  uint32_t ks_len;       /* ceil(bits(Q) / ks_bits) */
+  uint32_t ring_ternary; /* ring secret key: 1 ternary, 0 binary */
+  double lwe_noise_std;
+  double ring_noise_std;
+  double ks_noise_std;
+} hb_params;
+
+/* ---- parameters -------------------------------------------------------------------------- */
+
+/* Replaces the LazyLock parameter statics (tfhe/src/bfhe/parameters.rs:45-117). */
+int hb_params_preset(int preset, hb_params *out);
+/* Replaces Parameters::new's checks (fhe_core/src/parameter.rs:111-172). */
+int hb_params_validate(const hb_params *p);
+/* Word counts of the host buffers for p: lwe_sk, ring_sk, bsk, ksk, and one LWE ciphertext. */
+int hb_params_sizes(const hb_params *p, size_t *lwe_sk, size_t *ring_sk, size_t *bsk, size_t *ksk,
+                    size_t *lwe);
+
+/* ---- client side (host CPU) --------------------------------------------------------------- */
+
+/* KeyGen::generate_secret_key + Evaluator::new key material (tfhe/src/key_gen.rs:12,
+ * fhe_core/src/secret_key.rs:67-89, fhe_core/src/blind_rotation/rlwe/binary.rs:207-239,
+ * fhe_core/src/key_switch/rlwe.rs:37-112) from a 64-bit seed: the reference seeds from OS entropy,
+ * this library derives every sample from a counter PRG of (seed, stream, counter). */
+int hb_keygen(const hb_params *p, uint64_t seed, void *lwe_sk, void *ring_sk, void *bsk, void *ksk,
+              int threads);
+/* Encryptor::encrypt / SecretKeyPack::encrypt (fhe_core/src/secret_key.rs:129-149); ciphertext i
+ * uses sample index index0 + i. */
+int hb_encrypt(const hb_params *p, const void *lwe_sk, uint64_t seed, uint64_t index0,
+               const uint8_t *bits, size_t count, void *lwe_out);
+/* Decryptor::decrypt / SecretKeyPack::decrypt_with_noise (fhe_core/src/secret_key.rs:151-188);
+ * noise_out may be NULL. */
+int hb_decrypt(const hb_params *p, const void *lwe_sk, const void *lwe, size_t count,
+               uint8_t *bits_out, uint64_t *noise_out);
+
+/* ---- device context ----------------------------------------------------------------------- */
+
+/* One CUDA device, one stream, an HBM budget (bytes, 0 = unlimited) for key and batch memory. */
+int hb_ctx_create(int device, size_t hbm_budget, hb_ctx **out);
+void hb_ctx_destroy(hb_ctx *ctx);
+int hb_last_error(const hb_ctx *ctx, char *buf, size_t len);
+/* The context's cudaStream_t, for callers that enqueue their own copies around *_device calls. */
+int hb_ctx_stream(hb_ctx *ctx, void **stream);
+int hb_ctx_synchronize(hb_ctx *ctx);
+/* Bytes of device memory the context currently holds against its budget. */
+size_t hb_ctx_hbm_in_use(const hb_ctx *ctx);
+
+/* ---- evaluation keys (Evaluator::new, tfhe/src/bfhe/evaluate.rs:26-39) ---------------------- */
+
+/* Upload coefficient-domain BSK/KSK; transforms and lays them out on the device. */
+int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void *ksk, hb_keys **out);
+void hb_keys_free(hb_ctx *ctx, hb_keys *keys);
+int hb_keys_params(const hb_keys *keys, hb_params *out);
+
+/* ---- gate bootstrapping --------------------------------------------------------------------- */
+
+/* Evaluator::{nand,and,or,nor,xor,xnor,majority,not,mux} over `count` independent gates
+ * (tfhe/src/bfhe/evaluate.rs:98-262). c2 is read by MAJORITY and MUX only. Host buffers. */
+int hb_gate(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1, const void *c2,
+            void *out, size_t count);
+/* Same on device buffers, enqueued on the context stream (one persistent launch per bootstrap
+ * layer: MUX takes two). */
+int hb_gate_device(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1,
+                   const void *c2, void *out, size_t count);
+/* The plain form: one kernel launch per gate. */
+int hb_gate_device_plain(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1,
+                         void *out, size_t count);
+/* EvaluationKey::bootstrap(c, lut) (tfhe/src/bfhe/evaluate.rs:42-60) for count ciphertexts sharing
+ * one LUT polynomial of N words. Host buffers. */
+int hb_bootstrap_lut(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut, void *out,
+                     size_t count);
+
+/* ---- NTT table trait and external product (device slices) ---------------------------------- */
+
+/* AbstractNTT::transform_slice over count polynomials of 2^log_n words, in place. Output slot
+ * order is bit-reversed evaluation order at odd powers of a primitive 2N-th root (the reference's
+ * concrete-ntt order is unspecified; only round trips and products are part of the contract). */
+int hb_ntt_forward_device(hb_ctx *ctx, int field_id, uint32_t log_n, void *data, size_t count);
+/* AbstractNTT::inverse_transform_slice (inverse + normalise), in place. */
+int hb_ntt_inverse_device(hb_ctx *ctx, int field_id, uint32_t log_n, void *data, size_t count);
+/* Forward then inverse (round trip) from `in` to `out`. */
+int hb_ntt_roundtrip_device(hb_ctx *ctx, int field_id, uint32_t log_n, const void *in, void *out,
+                            size_t count);
+/* NTTRGSW from a coefficient-domain RGSW (host buffer, layout of one BSK entry); the returned
+ * device handle feeds hb_external_product_device and is released with hb_rgsw_free. */
+int hb_rgsw_upload(hb_ctx *ctx, int field_id, uint32_t log_n, uint32_t bits, uint32_t len,
+                   const void *rgsw, void **d_rgsw);
+void hb_rgsw_free(hb_ctx *ctx, void *d_rgsw);
+/* RLWE::mul_assign_ntt_rgsw (lattice/src/rlwe.rs:573-596): out_i = rlwe_i x RGSW for count
+ * coefficient-domain RLWEs (2 * 2^log_n words each). */
+int hb_external_product_device(hb_ctx *ctx, int field_id, uint32_t log_n, uint32_t bits,
+                               uint32_t len, const void *d_rgsw, const void *rlwe_in,
+                               void *rlwe_out, size_t count);
+
+/* ---- diagnostics ------------------------------------------------------------------------ */
+
+/* Field-multiplication throughput of this device (independent register chains, all SMs): the
+ * integer-pipe ceiling against which bootstrapping's modular multiplies are measured. No
+ * counterpart in the reference, which publishes CPU timings only. */
+int hb_probe_modmul(hb_ctx *ctx, int field_id, double *modmul_per_s);
+/* Kernel launches the context has issued for bootstrapping (batched and plain forms). */
+uint64_t hb_ctx_launches(const hb_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HB_GPU_H */

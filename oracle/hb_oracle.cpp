@@ -1,0 +1,1002 @@
+// hb_oracle.cpp -- TEST INFRASTRUCTURE ONLY (see hb_oracle.h for scope and parity status).
+//
+// CPU restatement of the reference's TFHE NAND/gate bootstrapping path. Every function cites
+// the reference file:line it follows. Arithmetic inside transforms is canonical; where the
+// reference's own code fixes a (possibly non-canonical) Goldilocks representation that can leak
+// into results -- accumulator additions and negations -- this file reproduces the reference's
+// exact u64 operations (algebra/src/modulus/goldilocks/ops.rs).
+//
+// Assumption (the reference's NTT lives in the un-vendored concrete-ntt crate): its forward and
+// inverse transforms are exact over Z/QZ and the inverse returns canonical values in [0, Q).
+
+#include "hb_oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace {
+
+typedef unsigned __int128 u128;
+
+// ------------------------------------------------------------------------------------------
+// Fields
+// ------------------------------------------------------------------------------------------
+
+// Goldilocks Q = 2^64 - 2^32 + 1 (algebra/src/modulus/goldilocks/mod.rs:9-11).
+struct Gold {
+  using T = uint64_t;
+  static constexpr T P = 0xFFFFFFFF00000001ULL;
+  static constexpr T EPS = 0xFFFFFFFFULL;  // 2^64 mod P
+  static constexpr int BITS = 64;          // bits(Q) (algebra/src/goldilocks/mod.rs:69-75)
+
+  static T canon(T x) { return x >= P ? x - P : x; }
+
+  // 128-bit -> 64-bit folding using 2^64 = 2^32 - 1 and 2^96 = -1 (mod P).
+  // Result in [0, 2^64), not necessarily canonical.
+  static T fold128(u128 x) {
+    T lo = (T)x;
+    T hi = (T)(x >> 64);
+    T hh = hi >> 32;
+    T hl = hi & EPS;
+    T t0 = lo - hh;
+    if (lo < hh) t0 -= EPS;  // wrapped by 2^64 (= EPS mod P): remove the EPS it added
+    T t1 = hl * EPS;
+    T r = t0 + t1;
+    if (r < t1) r += EPS;  // carry out of 2^64 is worth EPS; cannot carry twice
+    return r;
+  }
+
+  // Canonical arithmetic.
+  static T add(T a, T b) {
+    a = canon(a);
+    b = canon(b);
+    T s = a + b;
+    if (s < a || s >= P) s -= P;
+    return s;
+  }
+  static T sub(T a, T b) {
+    a = canon(a);
+    b = canon(b);
+    return a >= b ? a - b : a - b + P;
+  }
+  static T mul(T a, T b) { return canon(fold128((u128)a * b)); }
+  static T neg(T a) {
+    a = canon(a);
+    return a == 0 ? 0 : P - a;
+  }
+
+  // The reference's exact representation-level operations.
+  // add_reduce: algebra/src/modulus/goldilocks/ops.rs:26-35
+  static T add_ref(T a, T b) {
+    T s = a + b;
+    bool over = s < a;
+    T s2 = s + (over ? EPS : 0);
+    bool over2 = s2 < s;
+    if (over2) s2 += EPS;
+    return s2;
+  }
+  // sub_reduce: algebra/src/modulus/goldilocks/ops.rs:48-57
+  static T sub_ref(T a, T b) {
+    T d = a - b;
+    bool under = a < b;
+    T c = under ? EPS : 0;
+    T d2 = d - c;
+    bool under2 = d < c;
+    if (under2) d2 -= EPS;
+    return d2;
+  }
+  // neg_reduce: algebra/src/modulus/goldilocks/ops.rs:69-73 (`P - self`, wrapping when self > P)
+  static T neg_ref(T a) { return a == 0 ? 0 : P - a; }
+  // Field::value (algebra/src/goldilocks/mod.rs:53-56)
+  static T value(T a) { return canon(a); }
+  static T from_u64(uint64_t v) { return v; }  // Goldilocks::new stores the word unchanged
+};
+
+// BabyBear Q = 2^31 - 2^27 + 1 (algebra/src/modulus/baby_bear/mod.rs:11). The reference stores
+// Montgomery form; every operation on the path returns canonical residues, so the oracle works on
+// canonical values directly.
+struct Baby {
+  using T = uint32_t;
+  static constexpr T P = 0x78000001U;
+  static constexpr int BITS = 31;  // algebra/src/baby_bear/mod.rs:73-79
+
+  static T canon(T x) { return x % P; }
+  static T add(T a, T b) {
+    uint32_t s = a + b;  // a, b < 2^31
+    return s >= P ? s - P : s;
+  }
+  static T sub(T a, T b) { return a >= b ? a - b : a + P - b; }
+  static T mul(T a, T b) { return (T)(((uint64_t)a * b) % P); }
+  static T neg(T a) { return a == 0 ? 0 : P - a; }
+  static T add_ref(T a, T b) { return add(a, b); }  // ops.rs:9-17
+  static T sub_ref(T a, T b) { return sub(a, b); }  // ops.rs:28-35
+  static T neg_ref(T a) { return neg(a); }          // ops.rs:47-51
+  static T value(T a) { return a; }
+  static T from_u64(uint64_t v) { return (T)(v % P); }
+};
+
+template <class F>
+typename F::T fpow(typename F::T b, uint64_t e) {
+  typename F::T r = 1;
+  while (e) {
+    if (e & 1) r = F::mul(r, b);
+    b = F::mul(b, b);
+    e >>= 1;
+  }
+  return r;
+}
+
+template <class F>
+typename F::T finv(typename F::T a) {
+  return fpow<F>(a, (uint64_t)F::P - 2);
+}
+
+// ------------------------------------------------------------------------------------------
+// Negacyclic NTT (plain iterative radix-2, natural order in and out). Slot k holds the
+// evaluation at psi^(2k+1); the constant polynomial c transforms to [c; N], which is the
+// property the reference's key switch initialiser relies on (fhe_core/src/key_switch/rlwe.rs:118-121).
+// ------------------------------------------------------------------------------------------
+
+template <class F>
+struct Ntt {
+  using T = typename F::T;
+  uint32_t logn = 0, n = 0;
+  std::vector<T> psi_pow, psi_inv_pow, w_fwd, w_inv;  // w_*: cyclic roots per stage
+  T n_inv = 0;
+  bool ok = false;
+
+  explicit Ntt(uint32_t log_n) : logn(log_n), n(1u << log_n) {
+    uint64_t order = (uint64_t)F::P - 1;
+    if (order % (2ull * n) != 0) return;
+    T psi = 0;
+    for (T g = 2; g < 100; ++g) {
+      T c = fpow<F>(g, order / (2ull * n));
+      if (fpow<F>(c, n) == F::P - 1) {
+        psi = c;
+        break;
+      }
+    }
+    if (!psi) return;
+    T psi_inv = finv<F>(psi);
+    psi_pow.resize(n);
+    psi_inv_pow.resize(n);
+    T a = 1, b = 1;
+    for (uint32_t i = 0; i < n; ++i) {
+      psi_pow[i] = a;
+      psi_inv_pow[i] = b;
+      a = F::mul(a, psi);
+      b = F::mul(b, psi_inv);
+    }
+    T omega = F::mul(psi, psi), omega_inv = F::mul(psi_inv, psi_inv);
+    w_fwd.resize(n);
+    w_inv.resize(n);
+    // w_fwd[len/2 + j] = omega^(j * n/len) for stage of length len
+    for (uint32_t len = 2; len <= n; len <<= 1) {
+      T wl = fpow<F>(omega, n / len), wli = fpow<F>(omega_inv, n / len);
+      T x = 1, y = 1;
+      for (uint32_t j = 0; j < len / 2; ++j) {
+        w_fwd[len / 2 + j] = x;
+        w_inv[len / 2 + j] = y;
+        x = F::mul(x, wl);
+        y = F::mul(y, wli);
+      }
+    }
+    n_inv = finv<F>((T)n);
+    ok = true;
+  }
+
+  void cyclic(T *a, const std::vector<T> &w) const {
+    for (uint32_t i = 1, j = 0; i < n; ++i) {
+      uint32_t bit = n >> 1;
+      for (; j & bit; bit >>= 1) j ^= bit;
+      j ^= bit;
+      if (i < j) std::swap(a[i], a[j]);
+    }
+    for (uint32_t len = 2; len <= n; len <<= 1) {
+      uint32_t h = len / 2;
+      for (uint32_t i = 0; i < n; i += len) {
+        for (uint32_t j = 0; j < h; ++j) {
+          T u = a[i + j];
+          T v = F::mul(a[i + j + h], w[h + j]);
+          a[i + j] = F::add(u, v);
+          a[i + j + h] = F::sub(u, v);
+        }
+      }
+    }
+  }
+
+  // AbstractNTT::transform_slice (algebra/src/transformation/mod.rs:85)
+  void forward(T *a) const {
+    for (uint32_t i = 0; i < n; ++i) a[i] = F::mul(F::canon(a[i]), psi_pow[i]);
+    cyclic(a, w_fwd);
+  }
+  // AbstractNTT::inverse_transform_slice (algebra/src/transformation/mod.rs:95): inverse + normalize
+  void inverse(T *a) const {
+    for (uint32_t i = 0; i < n; ++i) a[i] = F::canon(a[i]);
+    cyclic(a, w_inv);
+    for (uint32_t i = 0; i < n; ++i) a[i] = F::mul(F::mul(a[i], n_inv), psi_inv_pow[i]);
+  }
+};
+
+template <class F>
+const Ntt<F> &ntt_table(uint32_t logn) {
+  // NTTField::get_ntt_table caches one table per log_n (algebra/src/goldilocks/goldilocks_ntt.rs:136-160)
+  static std::unique_ptr<Ntt<F>> tables[16];
+  static std::once_flag flags[16];
+  std::call_once(flags[logn], [&] { tables[logn].reset(new Ntt<F>(logn)); });
+  return *tables[logn];
+}
+
+template <class F>
+void schoolbook_negacyclic(const typename F::T *x, const typename F::T *y, typename F::T *out,
+                           uint32_t n) {
+  using T = typename F::T;
+  std::vector<T> acc(n, 0);
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t j = 0; j < n; ++j) {
+      T p = F::mul(x[i], y[j]);
+      uint32_t k = i + j;
+      if (k < n)
+        acc[k] = F::add(acc[k], p);
+      else
+        acc[k - n] = F::sub(acc[k - n], p);
+    }
+  std::copy(acc.begin(), acc.end(), out);
+}
+
+// ------------------------------------------------------------------------------------------
+// Seeded PRG and samplers (this build's key convention; the distributions follow
+// algebra/src/utils/sample.rs:6-51 and algebra/src/random.rs:82-96,156-171).
+// ------------------------------------------------------------------------------------------
+
+inline uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+inline uint64_t prg(uint64_t seed, uint64_t stream, uint64_t ctr) {
+  uint64_t k = mix64(seed + 0x9E3779B97F4A7C15ULL) ^ mix64(stream ^ 0xD1B54A32D192ED03ULL);
+  return mix64(k + ctr * 0x9E3779B97F4A7C15ULL);
+}
+
+enum : uint64_t { TAG_LWE_SK = 1, TAG_RING_SK = 2, TAG_BSK = 3, TAG_KSK = 4, TAG_ENC = 5 };
+
+inline uint64_t stream_id(uint64_t tag, uint64_t i, uint64_t part, uint64_t j, uint64_t which) {
+  return (tag << 56) | ((i & 0xFFFFFFFFULL) << 24) | ((part & 0xFF) << 16) | ((j & 0xFF) << 8) |
+         (which & 0xFF);
+}
+
+// Natural logarithm for s in (0, 1] from IEEE-exact operations only (frexp, +, -, *, /), so the
+// sampled noise is identical on every x86-64 host: ln s = e ln2 + 2 atanh((m-1)/(m+1)).
+double ln_exact(double s) {
+  int e = 0;
+  double m = std::frexp(s, &e);
+  if (m < 0.70710678118654752440) {
+    m *= 2.0;
+    e -= 1;
+  }
+  double y = (m - 1.0) / (m + 1.0);
+  double y2 = y * y;
+  double sum = 0.0, term = y;
+  for (int k = 0; k < 24; ++k) {
+    sum += term / (double)(2 * k + 1);
+    term *= y2;
+  }
+  return 2.0 * sum + (double)e * 0.693147180559945309417232121458;
+}
+
+inline double unit_double(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
+
+// FieldDiscreteGaussianSampler::sample (algebra/src/random.rs:156-171): N(0, sigma), reject
+// |x| >= 6 sigma, round half away from zero, negative r -> Q - |r|. The normal deviate comes from
+// the Marsaglia polar method on this build's PRG.
+template <class F>
+typename F::T gaussian(uint64_t seed, uint64_t stream, uint64_t coeff, double sigma) {
+  const double max_dev = sigma * 6.0;
+  for (uint64_t attempt = 0;; ++attempt) {
+    uint64_t base = (coeff << 20) | (attempt << 1);
+    double u = 2.0 * unit_double(prg(seed, stream, base)) - 1.0;
+    double v = 2.0 * unit_double(prg(seed, stream, base | 1)) - 1.0;
+    double s = u * u + v * v;
+    if (!(s > 0.0 && s < 1.0)) continue;
+    double x = u * std::sqrt(-2.0 * ln_exact(s) / s);
+    double value = sigma * x;
+    if (std::fabs(value) < max_dev) {
+      double r = std::round(value);
+      if (r < 0.0) return (typename F::T)((uint64_t)F::P - (uint64_t)(-r));
+      return (typename F::T)(uint64_t)r;
+    }
+  }
+}
+
+template <class F>
+typename F::T uniform(uint64_t seed, uint64_t stream, uint64_t k) {
+  return (typename F::T)(prg(seed, stream, k) % (uint64_t)F::P);
+}
+
+// ------------------------------------------------------------------------------------------
+// Parameters
+// ------------------------------------------------------------------------------------------
+
+struct Dims {
+  uint32_t N, logN, n, bits, len, ks_bits, ks_len;
+};
+
+bool dims_of(const orc_params *p, Dims &d) {
+  if (!p) return false;
+  d.N = p->ring_dim;
+  d.n = p->lwe_dim;
+  if (d.N < 2 || (d.N & (d.N - 1)) || d.N > 4096) return false;
+  d.logN = 0;
+  while ((1u << d.logN) < d.N) ++d.logN;
+  if (d.n == 0 || d.n > d.N) return false;
+  // key_switch_for_rlwe requires next_pow2(n) == N for the single-chunk path the paper sets take
+  uint32_t np2 = 1;
+  while (np2 < d.n) np2 <<= 1;
+  if (np2 != d.N) return false;
+  d.bits = p->br_bits;
+  d.len = p->br_len;
+  d.ks_bits = p->ks_bits;
+  d.ks_len = p->ks_len;
+  int fb = p->field_id == ORC_FIELD_GOLDILOCKS ? 64 : 31;
+  auto want = [&](uint32_t b) { return (uint32_t)((fb + (int)b - 1) / (int)b); };
+  if (d.bits == 0 || d.bits > 16 || d.len != want(d.bits)) return false;
+  if (d.ks_bits == 0 || d.ks_bits > 16 || d.ks_len != want(d.ks_bits)) return false;
+  return true;
+}
+
+// ------------------------------------------------------------------------------------------
+// Key generation (fhe_core/src/secret_key.rs:67-89, fhe_core/src/blind_rotation/rlwe/binary.rs:207-239,
+// lattice/src/rgsw.rs:343-395, lattice/src/gadget/rlwe.rs:478-552, lattice/src/rlwe.rs:1215-1252,
+// fhe_core/src/key_switch/rlwe.rs:37-112), restated in the coefficient domain.
+// ------------------------------------------------------------------------------------------
+
+template <class F>
+void negacyclic_mul(const Ntt<F> &ntt, const typename F::T *x, const typename F::T *y_ntt,
+                    typename F::T *out) {
+  std::vector<typename F::T> t(x, x + ntt.n);
+  ntt.forward(t.data());
+  for (uint32_t k = 0; k < ntt.n; ++k) t[k] = F::mul(t[k], y_ntt[k]);
+  ntt.inverse(t.data());
+  std::copy(t.begin(), t.end(), out);
+}
+
+template <class F>
+void rlwe_zero_sample(const Ntt<F> &ntt, const typename F::T *key_ntt, uint64_t seed,
+                      uint64_t stream_a, uint64_t stream_e, double sigma, typename F::T *a,
+                      typename F::T *b) {
+  // NTTRLWE::generate_random_zero_sample (lattice/src/rlwe.rs:1215-1230): b = a*s + e
+  uint32_t N = ntt.n;
+  for (uint32_t k = 0; k < N; ++k) a[k] = uniform<F>(seed, stream_a, k);
+  negacyclic_mul<F>(ntt, a, key_ntt, b);
+  for (uint32_t k = 0; k < N; ++k) b[k] = F::add(b[k], gaussian<F>(seed, stream_e, k, sigma));
+}
+
+template <class F>
+void keygen(const orc_params *p, const Dims &d, uint64_t seed, typename F::T *lwe_sk,
+            typename F::T *ring_sk, typename F::T *bsk, typename F::T *ksk, int threads) {
+  using T = typename F::T;
+  const uint32_t N = d.N, n = d.n;
+  const Ntt<F> &ntt = ntt_table<F>(d.logN);
+  // sample_binary_field_vec (algebra/src/utils/sample.rs:6-27)
+  for (uint32_t i = 0; i < n; ++i) lwe_sk[i] = (T)(prg(seed, stream_id(TAG_LWE_SK, 0, 0, 0, 0), i) & 1);
+  // sample_ternary_field_vec / random_with_binary (algebra/src/utils/sample.rs:30-51)
+  for (uint32_t k = 0; k < N; ++k) {
+    uint64_t r = prg(seed, stream_id(TAG_RING_SK, 0, 0, 0, 0), k);
+    if (p->ring_ternary) {
+      const T tbl[4] = {0, 0, 1, (T)(F::P - 1)};
+      ring_sk[k] = tbl[r & 3];
+    } else {
+      ring_sk[k] = (T)(r & 1);
+    }
+  }
+  std::vector<T> z_ntt(ring_sk, ring_sk + N);
+  ntt.forward(z_ntt.data());
+
+  const uint32_t L = d.len;
+  const size_t row = 2 * (size_t)N;            // one RLWE (a, b)
+  const size_t entry = 2 * (size_t)L * row;    // one RGSW = (c_neg_s_m, c_m)
+  auto work = [&](uint32_t i0, uint32_t i1) {
+    for (uint32_t i = i0; i < i1; ++i) {
+      const bool one = lwe_sk[i] != 0;
+      T basis_pow = 1;
+      for (uint32_t j = 0; j < L; ++j) {
+        for (uint32_t part = 0; part < 2; ++part) {
+          T *a = bsk + (size_t)i * entry + ((size_t)part * L + j) * row;
+          T *b = a + N;
+          rlwe_zero_sample<F>(ntt, z_ntt.data(), seed, stream_id(TAG_BSK, i, part, j, 0),
+                              stream_id(TAG_BSK, i, part, j, 1), p->ring_noise_std, a, b);
+          if (one && part == 0) {
+            // generate_random_neg_secret_sample: every NTT slot of a += B^j, i.e. a[0] += B^j
+            // (lattice/src/gadget/rlwe.rs:526-551)
+            a[0] = F::add(a[0], basis_pow);
+          } else if (one && part == 1) {
+            // generate_random_value_sample: e[0] += B^j before the transform (lattice/src/rlwe.rs:1233-1252)
+            b[0] = F::add(b[0], basis_pow);
+          }
+        }
+        // basis_power = lazy_new(basis_power.value() * basis) (lattice/src/gadget/rlwe.rs:518,546)
+        basis_pow = (T)((uint64_t)basis_pow << d.bits);
+      }
+    }
+  };
+  int nt = std::max(1, threads);
+  std::vector<std::thread> pool;
+  uint32_t chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    uint32_t i0 = t * chunk, i1 = std::min(n, i0 + chunk);
+    if (i0 >= i1) break;
+    pool.emplace_back(work, i0, i1);
+  }
+  for (auto &th : pool) th.join();
+
+  // KeySwitchingRLWEKey::generate (fhe_core/src/key_switch/rlwe.rs:37-112), next_pow2(n) == N branch:
+  // row j encrypts z * B_ks^j under the extended LWE key [s, 0...].
+  std::vector<T> s_ext(N, 0);
+  for (uint32_t i = 0; i < n; ++i) s_ext[i] = lwe_sk[i];
+  ntt.forward(s_ext.data());
+  std::vector<T> zk(ring_sk, ring_sk + N);
+  const T basis_ks = F::from_u64(1ull << d.ks_bits);
+  for (uint32_t j = 0; j < d.ks_len; ++j) {
+    T *a = ksk + (size_t)j * row;
+    T *b = a + N;
+    rlwe_zero_sample<F>(ntt, s_ext.data(), seed, stream_id(TAG_KSK, 0, 0, j, 0),
+                        stream_id(TAG_KSK, 0, 0, j, 1), p->ks_noise_std, a, b);
+    for (uint32_t k = 0; k < N; ++k) b[k] = F::add(b[k], zk[k]);
+    if (j + 1 < d.ks_len)
+      for (uint32_t k = 0; k < N; ++k) zk[k] = F::mul(zk[k], basis_ks);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Encode / decode / encrypt / decrypt (fhe_core/src/plaintext.rs:64-97, fhe_core/src/secret_key.rs:129-188)
+// ------------------------------------------------------------------------------------------
+
+template <class F>
+uint64_t encode(uint64_t m) {
+  double qf = (double)(uint64_t)F::P;
+  return (uint64_t)std::round((double)m * (qf / 4.0));
+}
+
+template <class F>
+uint64_t decode(uint64_t c) {
+  double qf = (double)(uint64_t)F::P;
+  uint64_t r = (uint64_t)std::round((double)c * 4.0 / qf);
+  return r < 4 ? r : r - 4;
+}
+
+template <class F>
+void encrypt(const Dims &d, const orc_params *p, const typename F::T *sk, uint64_t seed,
+             uint64_t index, int bit, typename F::T *out) {
+  using T = typename F::T;
+  // LWE::generate_random_zero_sample_field (lattice/src/lwe.rs:389-404)
+  T acc = 0;
+  for (uint32_t i = 0; i < d.n; ++i) {
+    out[i] = uniform<F>(seed, stream_id(TAG_ENC, index, 0, 0, 0), i);
+    acc = F::add(acc, F::mul(out[i], sk[i]));
+  }
+  T e = gaussian<F>(seed, stream_id(TAG_ENC, index, 0, 0, 1), 0, p->lwe_noise_std);
+  T b = F::add(acc, e);
+  out[d.n] = F::add(b, F::from_u64(encode<F>((uint64_t)bit)));
+}
+
+template <class F>
+void decrypt(const Dims &d, const typename F::T *sk, const typename F::T *c, uint8_t *bit,
+             uint64_t *noise) {
+  using T = typename F::T;
+  T acc = 0;
+  for (uint32_t i = 0; i < d.n; ++i) acc = F::add(acc, F::mul(F::canon(c[i]), sk[i]));
+  T pt = F::sub(F::canon(c[d.n]), acc);
+  uint64_t m = decode<F>(F::value(pt));
+  if (bit) *bit = (uint8_t)m;
+  if (noise) {
+    T fresh = F::from_u64(encode<F>(m));
+    T x = F::sub(pt, fresh), y = F::sub(fresh, pt);
+    *noise = std::min<uint64_t>(x, y);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Bootstrapping
+// ------------------------------------------------------------------------------------------
+
+template <class F>
+struct EvalKey {
+  using T = typename F::T;
+  Dims d;
+  std::vector<T> bsk_ntt;  // [i][part][j][ab][N] in this oracle's NTT domain
+  std::vector<T> ksk_ntt;  // [j][ab][N]
+};
+
+template <class F>
+EvalKey<F> *make_eval(const Dims &d, const typename F::T *bsk, const typename F::T *ksk,
+                      int threads) {
+  auto *ek = new EvalKey<F>();
+  ek->d = d;
+  const Ntt<F> &ntt = ntt_table<F>(d.logN);
+  size_t polys = (size_t)d.n * 2 * d.len * 2;
+  ek->bsk_ntt.assign(bsk, bsk + polys * d.N);
+  int nt = std::max(1, threads);
+  std::vector<std::thread> pool;
+  size_t chunk = (polys + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    size_t p0 = t * chunk, p1 = std::min(polys, p0 + chunk);
+    if (p0 >= p1) break;
+    pool.emplace_back([&, p0, p1] {
+      for (size_t q = p0; q < p1; ++q) ntt.forward(ek->bsk_ntt.data() + q * d.N);
+    });
+  }
+  for (auto &th : pool) th.join();
+  ek->ksk_ntt.assign(ksk, ksk + (size_t)d.ks_len * 2 * d.N);
+  for (size_t q = 0; q < (size_t)d.ks_len * 2; ++q) ntt.forward(ek->ksk_ntt.data() + q * d.N);
+  return ek;
+}
+
+// lwe_modulus_switch (fhe_core/src/modulus_switch.rs:12-38)
+template <class F>
+void modswitch(const Dims &d, const typename F::T *c, uint32_t *out) {
+  const double before = (double)(uint64_t)F::P;
+  const double after = (double)(2 * d.N);
+  for (uint32_t i = 0; i <= d.n; ++i) {
+    double v = (double)(uint64_t)F::value(c[i]);
+    double r = std::round(v * after / before);
+    uint64_t t = (uint64_t)r;
+    out[i] = (uint32_t)(t < 2ull * d.N ? t : t - 2ull * d.N);
+  }
+}
+
+// Polynomial::decompose_lsb_bits_inplace (algebra/src/polynomial/univariate/native_polynomial.rs:340-348)
+// with Goldilocks/BabyBear::decompose_lsb_bits_at (algebra/src/goldilocks/mod.rs:123-127,
+// algebra/src/baby_bear/mod.rs:127-131): digit = value & mask, poly = value >> bits.
+template <class F>
+void decompose_step(typename F::T *poly, typename F::T *digit, uint32_t N, uint32_t bits) {
+  const uint64_t mask = (1ull << bits) - 1;
+  for (uint32_t k = 0; k < N; ++k) {
+    uint64_t v = (uint64_t)F::value(poly[k]);
+    digit[k] = (typename F::T)(v & mask);
+    poly[k] = (typename F::T)(v >> bits);
+  }
+}
+
+// RLWE::mul_monic_monomial_sub_one_inplace (lattice/src/rlwe.rs:437-487): dst = src*(X^r - 1)
+template <class F>
+void monomial_sub_one(const typename F::T *y, typename F::T *x, uint32_t N, uint32_t r) {
+  if (r <= N) {
+    uint32_t nsr = N - r;
+    for (uint32_t k = 0; k < r; ++k) x[k] = F::neg_ref(y[nsr + k]);
+    for (uint32_t k = r; k < N; ++k) x[k] = y[k - r];
+  } else {
+    uint32_t rr = r - N;
+    uint32_t nsr = N - rr;
+    for (uint32_t k = 0; k < rr; ++k) x[k] = y[nsr + k];
+    for (uint32_t k = rr; k < N; ++k) x[k] = F::neg_ref(y[k - rr]);
+  }
+  for (uint32_t k = 0; k < N; ++k) x[k] = F::sub_ref(x[k], y[k]);
+}
+
+// RLWE::mul_assign_ntt_rgsw (lattice/src/rlwe.rs:573-596): c_neg_s_m x E.a + c_m x E.b, then INTT.
+// rgsw_ntt layout [part][j][ab][N].
+template <class F>
+void external_product(const Ntt<F> &ntt, uint32_t bits, uint32_t L, const typename F::T *rgsw_ntt,
+                      typename F::T *ea, typename F::T *eb) {
+  using T = typename F::T;
+  const uint32_t N = ntt.n;
+  std::vector<T> ma(N, 0), mb(N, 0), poly(N), digit(N);
+  for (uint32_t part = 0; part < 2; ++part) {
+    const T *src = part == 0 ? ea : eb;
+    std::copy(src, src + N, poly.begin());
+    for (uint32_t j = 0; j < L; ++j) {
+      decompose_step<F>(poly.data(), digit.data(), N, bits);
+      ntt.forward(digit.data());
+      const T *ka = rgsw_ntt + ((size_t)part * L + j) * 2 * N;
+      const T *kb = ka + N;
+      // ntt_add_mul_assign_fast (algebra/src/polynomial/univariate/ntt_polynomial.rs:620-629)
+      for (uint32_t k = 0; k < N; ++k) {
+        ma[k] = F::add(ma[k], F::mul(digit[k], ka[k]));
+        mb[k] = F::add(mb[k], F::mul(digit[k], kb[k]));
+      }
+    }
+  }
+  ntt.inverse(ma.data());
+  ntt.inverse(mb.data());
+  std::copy(ma.begin(), ma.end(), ea);
+  std::copy(mb.begin(), mb.end(), eb);
+}
+
+// BinaryBlindRotationKey::blind_rotate (fhe_core/src/blind_rotation/rlwe/binary.rs:28-104).
+// acc_a/acc_b hold the reference's representation of the accumulator.
+template <class F>
+void blind_rotate(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T *lut_in,
+                  uint32_t steps, typename F::T *acc_a, typename F::T *acc_b) {
+  using T = typename F::T;
+  const Dims &d = ek.d;
+  const uint32_t N = d.N;
+  const Ntt<F> &ntt = ntt_table<F>(d.logN);
+  std::vector<T> lut(lut_in, lut_in + N);
+  uint32_t b = ms[d.n];
+  if (b != 0) {
+    // lut * X^{-b} by rotate_right + negate (binary.rs:40-62)
+    uint32_t neg_b = 2 * N - b;
+    std::vector<T> t(N);
+    if (neg_b <= N) {
+      for (uint32_t k = 0; k < N; ++k) t[(k + neg_b) % N] = lut[k];
+      for (uint32_t k = 0; k < neg_b; ++k) t[k] = F::neg_ref(t[k]);
+    } else {
+      uint32_t r = neg_b - N;
+      for (uint32_t k = 0; k < N; ++k) t[(k + r) % N] = lut[k];
+      for (uint32_t k = r; k < N; ++k) t[k] = F::neg_ref(t[k]);
+    }
+    lut.swap(t);
+  }
+  std::fill(acc_a, acc_a + N, (T)0);
+  std::copy(lut.begin(), lut.end(), acc_b);
+  std::vector<T> ea(N), eb(N);
+  const size_t entry = (size_t)2 * d.len * 2 * N;
+  for (uint32_t i = 0; i < d.n && i < steps; ++i) {
+    uint32_t ai = ms[i];
+    if (ai == 0) continue;  // binary.rs:70
+    monomial_sub_one<F>(acc_a, ea.data(), N, ai);
+    monomial_sub_one<F>(acc_b, eb.data(), N, ai);
+    external_product<F>(ntt, d.bits, d.len, ek.bsk_ntt.data() + i * entry, ea.data(), eb.data());
+    // RLWE::add_assign_element_wise (lattice/src/rlwe.rs:287-290)
+    for (uint32_t k = 0; k < N; ++k) {
+      acc_a[k] = F::add_ref(acc_a[k], ea[k]);
+      acc_b[k] = F::add_ref(acc_b[k], eb[k]);
+    }
+  }
+}
+
+// KeySwitchingRLWEKey::key_switch_for_rlwe (fhe_core/src/key_switch/rlwe.rs:115-137) with
+// key_switch_inner (SubAMulS, :250-286) and extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402).
+template <class F>
+void key_switch(const EvalKey<F> &ek, const typename F::T *acc_a, const typename F::T *acc_b,
+                typename F::T *out) {
+  using T = typename F::T;
+  const Dims &d = ek.d;
+  const uint32_t N = d.N;
+  const Ntt<F> &ntt = ntt_table<F>(d.logN);
+  std::vector<T> ia(N, 0), ib(N, F::canon(acc_b[0]));  // NTTRLWE(0, [b0; N])
+  std::vector<T> poly(N), digit(N);
+  // sub_assign_gadget_rlwe_mul_polynomial_inplace_fast (lattice/src/rlwe.rs:1147-1166): negate, then add
+  for (uint32_t k = 0; k < N; ++k) poly[k] = F::neg_ref(acc_a[k]);
+  for (uint32_t j = 0; j < d.ks_len; ++j) {
+    decompose_step<F>(poly.data(), digit.data(), N, d.ks_bits);
+    ntt.forward(digit.data());
+    const T *ka = ek.ksk_ntt.data() + (size_t)j * 2 * N;
+    const T *kb = ka + N;
+    for (uint32_t k = 0; k < N; ++k) {
+      ia[k] = F::add(ia[k], F::mul(digit[k], ka[k]));
+      ib[k] = F::add(ib[k], F::mul(digit[k], kb[k]));
+    }
+  }
+  ntt.inverse(ia.data());
+  ntt.inverse(ib.data());
+  out[0] = ia[0];
+  for (uint32_t k = 1; k < d.n; ++k) out[k] = F::neg_ref(ia[N - k]);
+  out[d.n] = ib[0];
+}
+
+// EvaluationKey::bootstrap (tfhe/src/bfhe/evaluate.rs:42-60)
+template <class F>
+void bootstrap(const EvalKey<F> &ek, const typename F::T *c, const typename F::T *lut,
+               typename F::T *out) {
+  using T = typename F::T;
+  const Dims &d = ek.d;
+  std::vector<uint32_t> ms(d.n + 1);
+  modswitch<F>(d, c, ms.data());
+  std::vector<T> acc_a(d.N), acc_b(d.N);
+  blind_rotate<F>(ek, ms.data(), lut, d.n, acc_a.data(), acc_b.data());
+  acc_b[0] = F::add_ref(acc_b[0], (T)((uint64_t)F::P >> 3));  // evaluate.rs:52
+  key_switch<F>(ek, acc_a.data(), acc_b.data(), out);
+}
+
+// LUT builders (tfhe/src/bfhe/evaluate.rs:267-465) with lut_step 1.
+template <class F>
+void make_lut(int gate, uint32_t N, typename F::T *lut) {
+  using T = typename F::T;
+  const T q8 = (T)((uint64_t)F::P >> 3);
+  const T nq8 = (T)((uint64_t)F::P - q8);
+  T lo, hi;
+  uint32_t mid;
+  switch (gate) {
+    case ORC_GATE_NAND: mid = N / 2 + N / 4; lo = q8; hi = nq8; break;
+    case ORC_GATE_AND:
+    case ORC_GATE_MAJORITY: mid = N / 2 + N / 4; lo = nq8; hi = q8; break;
+    case ORC_GATE_OR:
+    case ORC_GATE_MUX: mid = N / 4; lo = nq8; hi = q8; break;
+    case ORC_GATE_NOR: mid = N / 4; lo = q8; hi = nq8; break;
+    case ORC_GATE_XOR: mid = N / 2; lo = nq8; hi = q8; break;
+    case ORC_GATE_XNOR: mid = N / 2; lo = q8; hi = nq8; break;
+    default: mid = N; lo = 0; hi = 0;
+  }
+  for (uint32_t k = 0; k < N; ++k) lut[k] = k < mid ? lo : hi;
+}
+
+// Evaluator gate front-ends (tfhe/src/bfhe/evaluate.rs:98-262).
+template <class F>
+void gate_one(const EvalKey<F> &ek, int gate, const typename F::T *c0, const typename F::T *c1,
+              const typename F::T *c2, typename F::T *out) {
+  using T = typename F::T;
+  const Dims &d = ek.d;
+  const uint32_t m = d.n + 1;
+  std::vector<T> c(m), lut(d.N);
+  auto not_ = [&](const T *x, T *y) {  // evaluate.rs:98-105
+    for (uint32_t i = 0; i < m; ++i) y[i] = F::neg(x[i]);
+    y[d.n] = F::add(y[d.n], (T)((uint64_t)F::P >> 2));
+  };
+  switch (gate) {
+    case ORC_GATE_NOT:
+      not_(c0, out);
+      return;
+    case ORC_GATE_NAND:
+    case ORC_GATE_AND:
+    case ORC_GATE_OR:
+    case ORC_GATE_NOR:
+      for (uint32_t i = 0; i < m; ++i) c[i] = F::add(c0[i], c1[i]);
+      break;
+    case ORC_GATE_XOR:
+    case ORC_GATE_XNOR:
+      for (uint32_t i = 0; i < m; ++i) {
+        T s = F::sub(c0[i], c1[i]);
+        c[i] = F::add(s, s);
+      }
+      break;
+    case ORC_GATE_MAJORITY:
+      for (uint32_t i = 0; i < m; ++i) c[i] = F::add(F::add(c0[i], c1[i]), c2[i]);
+      break;
+    case ORC_GATE_MUX: {  // evaluate.rs:245-262
+      std::vector<T> nc0(m), t0(m), t1(m);
+      not_(c0, nc0.data());
+      gate_one<F>(ek, ORC_GATE_AND, c0, c1, nullptr, t0.data());
+      gate_one<F>(ek, ORC_GATE_AND, nc0.data(), c2, nullptr, t1.data());
+      for (uint32_t i = 0; i < m; ++i) c[i] = F::add(t0[i], t1[i]);
+      break;
+    }
+    default:
+      return;
+  }
+  make_lut<F>(gate, d.N, lut.data());
+  bootstrap<F>(ek, c.data(), lut.data(), out);
+}
+
+template <class Fn>
+void parallel_for(size_t count, int threads, Fn fn) {
+  int nt = (int)std::min<size_t>(std::max(1, threads), std::max<size_t>(count, 1));
+  if (nt <= 1) {
+    for (size_t i = 0; i < count; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  std::atomic<size_t> next{0};
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&] {
+      for (size_t i; (i = next.fetch_add(1)) < count;) fn(i);
+    });
+  for (auto &th : pool) th.join();
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// C API
+// ------------------------------------------------------------------------------------------
+
+extern "C" {
+
+int orc_params_preset(int preset, orc_params *out) {
+  if (!out) return -1;
+  std::memset(out, 0, sizeof(*out));
+  out->ring_dim = 1024;
+  out->lwe_dim = 728;
+  out->ring_ternary = 1;
+  out->ks_bits = 5;
+  switch (preset) {
+    case 0:  // BABYBEAR_BINARY_128_BITS_PARAMETERS (tfhe/src/bfhe/parameters.rs:45-61)
+      out->field_id = ORC_FIELD_BABYBEAR;
+      out->br_bits = 8;
+      out->br_len = 4;
+      out->ks_len = 7;
+      out->lwe_noise_std = 11000.0;
+      out->ring_noise_std = 41.9;
+      out->ks_noise_std = 11000.0;
+      return 0;
+    case 1:  // GOLDILOCKS_BINARY_128_BITS_PARAMETERS (tfhe/src/bfhe/parameters.rs:64-80)
+    case 2:  // ZAMA_BINARY_128_BITS_PARAMETERS (tfhe/src/bfhe/parameters.rs:83-98)
+      out->field_id = ORC_FIELD_GOLDILOCKS;
+      out->br_bits = preset == 1 ? 8 : 5;
+      out->br_len = preset == 1 ? 8 : 13;
+      out->ks_len = 13;
+      out->lwe_noise_std = 2.9 * (double)(1ULL << 45);
+      out->ring_noise_std = 2.3 * (double)(1ULL << 37);
+      out->ks_noise_std = 2.9 * (double)(1ULL << 45);
+      return 0;
+    default:
+      return -1;
+  }
+}
+
+uint64_t orc_prg(uint64_t seed, uint64_t stream, uint64_t ctr) { return prg(seed, stream, ctr); }
+
+#define ORC_DISPATCH(p, BODY)                                  \
+  do {                                                         \
+    if ((p)->field_id == ORC_FIELD_GOLDILOCKS) {               \
+      using F = Gold;                                          \
+      BODY;                                                    \
+    } else if ((p)->field_id == ORC_FIELD_BABYBEAR) {          \
+      using F = Baby;                                          \
+      BODY;                                                    \
+    } else {                                                   \
+      return -1;                                               \
+    }                                                          \
+  } while (0)
+
+int orc_keygen(const orc_params *p, uint64_t seed, void *lwe_sk, void *ring_sk, void *bsk,
+               void *ksk, int threads) {
+  Dims d;
+  if (!dims_of(p, d) || !lwe_sk || !ring_sk || !bsk || !ksk) return -1;
+  ORC_DISPATCH(p, {
+    using T = F::T;
+    keygen<F>(p, d, seed, (T *)lwe_sk, (T *)ring_sk, (T *)bsk, (T *)ksk, threads);
+  });
+  return 0;
+}
+
+int orc_encrypt(const orc_params *p, const void *lwe_sk, uint64_t seed, uint64_t index0,
+                const uint8_t *bits, size_t count, void *lwe_out) {
+  Dims d;
+  if (!dims_of(p, d)) return -1;
+  ORC_DISPATCH(p, {
+    using T = F::T;
+    for (size_t i = 0; i < count; ++i)
+      encrypt<F>(d, p, (const T *)lwe_sk, seed, index0 + i, bits[i] & 1,
+                 (T *)lwe_out + i * (d.n + 1));
+  });
+  return 0;
+}
+
+int orc_decrypt(const orc_params *p, const void *lwe_sk, const void *lwe, size_t count,
+                uint8_t *bits_out, uint64_t *noise_out) {
+  Dims d;
+  if (!dims_of(p, d)) return -1;
+  ORC_DISPATCH(p, {
+    using T = F::T;
+    for (size_t i = 0; i < count; ++i)
+      decrypt<F>(d, (const T *)lwe_sk, (const T *)lwe + i * (d.n + 1),
+                 bits_out ? bits_out + i : nullptr, noise_out ? noise_out + i : nullptr);
+  });
+  return 0;
+}
+
+int orc_gate(const orc_params *p, const void *bsk, const void *ksk, int gate, const void *c0,
+             const void *c1, const void *c2, void *out, size_t count, int threads) {
+  Dims d;
+  if (!dims_of(p, d) || gate < 0 || gate > ORC_GATE_MUX) return -1;
+  if ((gate == ORC_GATE_MAJORITY || gate == ORC_GATE_MUX) && !c2) return -1;
+  ORC_DISPATCH(p, {
+    using T = F::T;
+    std::unique_ptr<EvalKey<F>> ek(make_eval<F>(d, (const T *)bsk, (const T *)ksk, threads));
+    const size_t m = d.n + 1;
+    parallel_for(count, threads, [&](size_t i) {
+      gate_one<F>(*ek, gate, (const T *)c0 + i * m, c1 ? (const T *)c1 + i * m : nullptr,
+                  c2 ? (const T *)c2 + i * m : nullptr, (T *)out + i * m);
+    });
+  });
+  return 0;
+}
+
+int orc_bootstrap_lut(const orc_params *p, const void *bsk, const void *ksk, const void *c,
+                      const void *lut, void *out, size_t count, int threads) {
+  Dims d;
+  if (!dims_of(p, d)) return -1;
+  ORC_DISPATCH(p, {
+    using T = F::T;
+    std::unique_ptr<EvalKey<F>> ek(make_eval<F>(d, (const T *)bsk, (const T *)ksk, threads));
+    const size_t m = d.n + 1;
+    parallel_for(count, threads, [&](size_t i) {
+      bootstrap<F>(*ek, (const T *)c + i * m, (const T *)lut, (T *)out + i * m);
+    });
+  });
+  return 0;
+}
+
+int orc_modswitch(const orc_params *p, const void *c, uint32_t *out) {
+  Dims d;
+  if (!dims_of(p, d)) return -1;
+  ORC_DISPATCH(p, { modswitch<F>(d, (const F::T *)c, out); });
+  return 0;
+}
+
+int orc_blind_rotate(const orc_params *p, const void *bsk, const void *c, const void *lut,
+                     uint32_t steps, void *acc_out) {
+  Dims d;
+  if (!dims_of(p, d)) return -1;
+  ORC_DISPATCH(p, {
+    using T = F::T;
+    // only the first `steps` BSK entries are needed: transform just those
+    Dims dd = d;
+    std::unique_ptr<EvalKey<F>> ek(new EvalKey<F>());
+    ek->d = dd;
+    const Ntt<F> &ntt = ntt_table<F>(d.logN);
+    uint32_t used = std::min(steps, d.n);
+    size_t entry = (size_t)2 * d.len * 2 * d.N;
+    ek->bsk_ntt.assign((const T *)bsk, (const T *)bsk + used * entry);
+    for (size_t q = 0; q < used * (size_t)2 * d.len * 2; ++q)
+      ntt.forward(ek->bsk_ntt.data() + q * d.N);
+    std::vector<uint32_t> ms(d.n + 1);
+    modswitch<F>(d, (const T *)c, ms.data());
+    T *acc = (T *)acc_out;
+    blind_rotate<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N);
+    for (uint32_t k = 0; k < 2 * d.N; ++k) acc[k] = F::canon(acc[k]);
+  });
+  return 0;
+}
+
+int orc_ntt_roundtrip(int field_id, uint32_t log_n, const void *in, void *out) {
+  if (log_n < 1 || log_n > 15) return -1;
+  orc_params p;
+  p.field_id = field_id;
+  ORC_DISPATCH(&p, {
+    using T = F::T;
+    const Ntt<F> &ntt = ntt_table<F>(log_n);
+    if (!ntt.ok) return -1;
+    std::vector<T> t((const T *)in, (const T *)in + ntt.n);
+    ntt.forward(t.data());
+    ntt.inverse(t.data());
+    std::copy(t.begin(), t.end(), (T *)out);
+  });
+  return 0;
+}
+
+int orc_negacyclic_mul(int field_id, uint32_t log_n, const void *x, const void *y, void *out,
+                       int schoolbook) {
+  if (log_n < 1 || log_n > 15) return -1;
+  orc_params p;
+  p.field_id = field_id;
+  ORC_DISPATCH(&p, {
+    using T = F::T;
+    const uint32_t n = 1u << log_n;
+    if (schoolbook) {
+      schoolbook_negacyclic<F>((const T *)x, (const T *)y, (T *)out, n);
+    } else {
+      const Ntt<F> &ntt = ntt_table<F>(log_n);
+      if (!ntt.ok) return -1;
+      std::vector<T> yy((const T *)y, (const T *)y + n);
+      ntt.forward(yy.data());
+      negacyclic_mul<F>(ntt, (const T *)x, yy.data(), (T *)out);
+    }
+  });
+  return 0;
+}
+
+int orc_external_product(int field_id, uint32_t log_n, uint32_t bits, uint32_t len,
+                         const void *rlwe, const void *rgsw, void *out, size_t count,
+                         int threads) {
+  if (log_n < 1 || log_n > 15 || bits == 0 || bits > 16 || len == 0) return -1;
+  orc_params p;
+  p.field_id = field_id;
+  ORC_DISPATCH(&p, {
+    using T = F::T;
+    const Ntt<F> &ntt = ntt_table<F>(log_n);
+    if (!ntt.ok) return -1;
+    const uint32_t n = 1u << log_n;
+    std::vector<T> k((const T *)rgsw, (const T *)rgsw + (size_t)2 * len * 2 * n);
+    for (size_t q = 0; q < (size_t)2 * len * 2; ++q) ntt.forward(k.data() + q * n);
+    parallel_for(count, threads, [&](size_t i) {
+      std::vector<T> a((const T *)rlwe + i * 2 * n, (const T *)rlwe + i * 2 * n + n);
+      std::vector<T> b((const T *)rlwe + i * 2 * n + n, (const T *)rlwe + (i + 1) * 2 * n);
+      external_product<F>(ntt, bits, len, k.data(), a.data(), b.data());
+      std::copy(a.begin(), a.end(), (T *)out + i * 2 * n);
+      std::copy(b.begin(), b.end(), (T *)out + i * 2 * n + n);
+    });
+  });
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+"""Generate the golden fixtures of tests/golden/ with the CPU oracle.
+
+    python tests/golden/gen_golden.py
+
+For each parameter set (BABYBEAR / GOLDILOCKS / ZAMA _BINARY_128_BITS) with key seed 0 it records:
+SHA-256 digests of the secret keys, BSK and KSK (this build's seeded key convention); the input
+ciphertexts of the four NAND truth-table rows (encryption seed 0, sample indices 0..7); the oracle's
+NAND outputs. The BabyBear set also records every other gate, a caller-LUT bootstrap, the modulus
+switch of the first NAND input and the blind-rotation accumulator after 1, 2 and 10 steps.
+The reference ships no golden vectors (its tests draw from OS entropy), so these files pin the
+oracle and the GPU path against each other and against regressions.
+"""
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import binding as O  # noqa: E402
+
+ROWS = np.array([[0, 0], [0, 1], [1, 0], [1, 1]], np.uint8)
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main():
+    out = {}
+    for pid, name in O.PRESET_NAMES.items():
+        p = O.preset(pid)
+        k = O.keygen(p, 0)
+        out[f"{name}/sha_lwe_sk"] = np.array(digest(k.lwe_sk))
+        out[f"{name}/sha_ring_sk"] = np.array(digest(k.ring_sk))
+        out[f"{name}/sha_bsk"] = np.array(digest(k.bsk))
+        out[f"{name}/sha_ksk"] = np.array(digest(k.ksk))
+        c0 = O.encrypt(p, k.lwe_sk, 0, 0, ROWS[:, 0])
+        c1 = O.encrypt(p, k.lwe_sk, 0, 4, ROWS[:, 1])
+        out[f"{name}/c0"] = c0
+        out[f"{name}/c1"] = c1
+        out[f"{name}/nand"] = O.gate(k, "nand", c0, c1)
+        if pid == O.PRESET_BABYBEAR:
+            c2 = O.encrypt(p, k.lwe_sk, 0, 8, np.array([1, 0, 1, 0], np.uint8))
+            out[f"{name}/c2"] = c2
+            for g in ("and", "or", "nor", "xor", "xnor"):
+                out[f"{name}/{g}"] = O.gate(k, g, c0, c1)
+            out[f"{name}/majority"] = O.gate(k, "majority", c0, c1, c2)
+            out[f"{name}/mux"] = O.gate(k, "mux", c0, c1, c2)
+            out[f"{name}/not"] = O.gate(k, "not", c0)
+            lut = (np.random.default_rng(11).integers(0, O.MODULUS[p.field_id], p.ring_dim,
+                                                       dtype=np.uint64)).astype(np.uint32)
+            out[f"{name}/lut"] = lut
+            out[f"{name}/bootstrap_lut"] = O.bootstrap_lut(k, c0, lut)
+            s = (c0[0].astype(np.uint64) + c1[0].astype(np.uint64)) % O.MODULUS[p.field_id]
+            s = s.astype(np.uint32)
+            out[f"{name}/ms0"] = O.modswitch(p, s)
+            nl = O.lut_poly(p.field_id, "nand", p.ring_dim)
+            for steps in (1, 2, 10):
+                out[f"{name}/acc{steps}"] = O.blind_rotate(k, s, nl, steps)
+    np.savez_compressed(os.path.join(HERE, "golden_seed0.npz"), **out)
+    print("wrote", os.path.join(HERE, "golden_seed0.npz"), len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,63 @@
+"""Host-side client code of the product (keygen / encrypt / decrypt) against the oracle."""
+
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_seed0.npz")
+
+
+@pytest.mark.parametrize("pid", [0, 1, 2])
+def test_product_keygen_matches_oracle(hb, oracle, oracle_keys, pid):
+    p = hb.Parameters.preset(pid)
+    sk = hb.KeyGen.generate_secret_key(p, 0)
+    bsk, ksk = sk.evaluation_key_material()
+    k = oracle_keys(pid)
+    assert (sk.lwe_secret_key == k.lwe_sk).all()
+    assert (sk.ring_secret_key == k.ring_sk).all()
+    assert (bsk == k.bsk).all()
+    assert (ksk == k.ksk).all()
+    g = np.load(GOLDEN)
+    name = oracle.PRESET_NAMES[pid]
+    assert hashlib.sha256(bsk.tobytes()).hexdigest() == str(g[f"{name}/sha_bsk"])
+
+
+@pytest.mark.parametrize("pid", [0, 1, 2])
+def test_encrypt_decrypt_matches_oracle(hb, oracle, oracle_keys, pid):
+    p = hb.Parameters.preset(pid)
+    sk = hb.SecretKeyPack(p, 0)
+    bits = np.random.default_rng(pid).integers(0, 2, 64).astype(np.uint8)
+    c = sk.encrypt(bits, index0=100)
+    k = oracle_keys(pid)
+    assert (c == oracle.encrypt(k.p, k.lwe_sk, 0, 100, bits)).all()
+    m, noise = sk.decrypt_with_noise(c)
+    mo, noiseo = oracle.decrypt(k.p, k.lwe_sk, c)
+    assert (m == bits).all() and (mo == bits).all() and (noise == noiseo).all()
+    g = np.load(GOLDEN)
+    name = oracle.PRESET_NAMES[pid]
+    assert (sk.encrypt([0, 0, 1, 1], 0) == g[f"{name}/c0"]).all()
+
+
+def test_parameter_validation(hb):
+    from hasteboots_b200._lib import HbError, HbParams, lib
+    import ctypes
+    raw = HbParams()
+    assert lib().hb_params_preset(1, ctypes.byref(raw)) == 0
+    assert lib().hb_params_validate(ctypes.byref(raw)) == 0
+    bad = [("ring_dim", 1000), ("lwe_dim", 300), ("br_len", 7), ("br_bits", 0), ("field_id", 5),
+           ("ring_dim", 8192)]
+    for field, value in bad:
+        r = HbParams()
+        lib().hb_params_preset(1, ctypes.byref(r))
+        setattr(r, field, value)
+        assert lib().hb_params_validate(ctypes.byref(r)) == -1, field
+    with pytest.raises(HbError):
+        hb.Parameters(bad_params())
+    assert lib().hb_params_preset(9, ctypes.byref(raw)) == -1
+
+
+def bad_params():
+    from hasteboots_b200._lib import HbParams
+    return HbParams()

@@ -1,0 +1,104 @@
+"""The CPU oracle against the reference's own known-answer tests and properties, and against the
+committed golden fixtures (tests/golden/gen_golden.py)."""
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rng
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_seed0.npz")
+FIELDS = [0, 1]
+
+
+def rand_poly(oracle, field, n, seed):
+    q = oracle.MODULUS[field]
+    return (rng(seed).integers(0, 2**63, n, dtype=np.uint64) % np.uint64(q)).astype(
+        oracle.dtype_of(field))
+
+
+@pytest.mark.parametrize("field", FIELDS)
+def test_monomial_products_kat(oracle, field):
+    # algebra/src/baby_bear/babybear_ntt.rs:185-213: 37 X^50 * 67 X^70 = 2479 X^120,
+    # and * 55 X^90 = 136345 X^210
+    dt = oracle.dtype_of(field)
+    p1, p2, p3 = (np.zeros(1024, dt) for _ in range(3))
+    p1[50], p2[70], p3[90] = 37, 67, 55
+    prod = oracle.negacyclic_mul(field, 10, p1, p2)
+    expect = np.zeros(1024, dt)
+    expect[120] = 37 * 67
+    assert (prod == expect).all()
+    prod3 = oracle.negacyclic_mul(field, 10, prod, p3)
+    expect3 = np.zeros(1024, dt)
+    expect3[210] = 37 * 67 * 55
+    assert (prod3 == expect3).all()
+    # wrap-around is negacyclic: X^600 * X^600 = -X^176
+    a = np.zeros(1024, dt)
+    a[600] = 1
+    w = oracle.negacyclic_mul(field, 10, a, a)
+    assert w[176] == oracle.MODULUS[field] - 1 and np.count_nonzero(w) == 1
+
+
+@pytest.mark.parametrize("field", FIELDS)
+@pytest.mark.parametrize("log_n", [5, 10, 11])
+def test_ntt_roundtrip_and_schoolbook(oracle, field, log_n):
+    # goldilocks_ntt.rs:173-183 / babybear_ntt.rs:169-182 round trips; polynomial_test.rs:110-154
+    n = 1 << log_n
+    x = rand_poly(oracle, field, n, 1 + log_n)
+    y = rand_poly(oracle, field, n, 2 + log_n)
+    assert (oracle.ntt_roundtrip(field, log_n, x) == x).all()
+    if log_n <= 10:
+        assert (oracle.negacyclic_mul(field, log_n, x, y) ==
+                oracle.negacyclic_mul(field, log_n, x, y, schoolbook=True)).all()
+
+
+@pytest.mark.parametrize("field,bits,length", [(1, 5, 13), (1, 8, 8), (0, 8, 4), (0, 5, 7)])
+def test_external_product_vs_plaintext(oracle, field, bits, length):
+    # lattice/tests/lattice_test.rs:352-406: RGSW(m) x RLWE(p) decrypts to m*p. With a noiseless
+    # "RGSW" of message 1 under key 0 (c_m rows = (0, B^j), c_neg_s_m rows = (B^j, 0)) the external
+    # product must reproduce the input exactly (gadget recomposition).
+    n = 64
+    dt = oracle.dtype_of(field)
+    rgsw = np.zeros((2, length, 2, n), dt)
+    for j in range(length):
+        rgsw[0, j, 0, 0] = 1 << (bits * j)
+        rgsw[1, j, 1, 0] = 1 << (bits * j)
+    rl = np.stack([rand_poly(oracle, field, 2 * n, 5)]).reshape(1, 2 * n)
+    out = oracle.external_product(field, 6, bits, length, rl, rgsw.reshape(-1))
+    assert (out == rl).all()
+
+
+def test_keygen_deterministic_and_truth_tables(oracle, oracle_keys):
+    p = oracle.preset(0)
+    k = oracle_keys(0)
+    k2 = oracle.keygen(p, 0, threads=3)
+    assert (k.bsk == k2.bsk).all() and (k.ksk == k2.ksk).all()
+    assert set(np.unique(k.lwe_sk)) <= {0, 1}
+    assert set(np.unique(k.ring_sk)) <= {0, 1, oracle.MODULUS[0] - 1}
+    bits = np.array([0, 0, 1, 1], np.uint8), np.array([0, 1, 0, 1], np.uint8)
+    c0 = oracle.encrypt(p, k.lwe_sk, 3, 0, bits[0])
+    c1 = oracle.encrypt(p, k.lwe_sk, 3, 4, bits[1])
+    tables = {"nand": lambda a, b: 1 - (a & b), "and": lambda a, b: a & b, "or": lambda a, b: a | b,
+              "nor": lambda a, b: 1 - (a | b), "xor": lambda a, b: a ^ b,
+              "xnor": lambda a, b: 1 - (a ^ b)}
+    q = oracle.MODULUS[0]
+    for g, f in tables.items():
+        m, noise = oracle.decrypt(p, k.lwe_sk, oracle.gate(k, g, c0, c1))
+        assert (m == f(*bits)).all(), g
+        assert (noise < q // 16).all(), g  # tfhe/examples/nand_babybear.rs:16-24
+
+
+def test_golden_fixtures_reproduce(oracle, oracle_keys):
+    import hashlib
+    g = np.load(GOLDEN)
+    for pid, name in oracle.PRESET_NAMES.items():
+        k = oracle_keys(pid)
+        assert hashlib.sha256(k.bsk.tobytes()).hexdigest() == str(g[f"{name}/sha_bsk"])
+        assert hashlib.sha256(k.ksk.tobytes()).hexdigest() == str(g[f"{name}/sha_ksk"])
+        if pid == 0:  # full bootstrap re-run on the fast set; the others are checked on the GPU
+            out = oracle.gate(k, "nand", g[f"{name}/c0"], g[f"{name}/c1"])
+            assert (out == g[f"{name}/nand"]).all()
+        m, noise = oracle.decrypt(k.p, k.lwe_sk, g[f"{name}/nand"])
+        assert (m == [1, 1, 1, 0]).all()
+        assert (noise < oracle.MODULUS[k.p.field_id] // 16).all()
