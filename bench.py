@@ -254,12 +254,15 @@ def main():
     pin1 = torch.from_numpy(c1.view(np.int64).copy()).pin_memory()
     pout = torch.zeros_like(pin0).pin_memory()
     e2e_times = []
-    for s in range(args.e2e_steps + 1):
+    for s in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         a0 = time.perf_counter()
         check(L.hb_gate(ctx.handle, ev.keys.handle, GATE_NAND, pin0.data_ptr(), pin1.data_ptr(), None,
                         pout.data_ptr(), G), "hb_gate", ctx.handle)
         if s > 0:
             e2e_times.append(time.perf_counter() - a0)
+    if not e2e_times:  # e2e leg disabled (profiling runs): reuse the device outputs
+        pout.copy_(torch.from_numpy(out.view(np.int64)))
+        e2e_times = [float("nan")]
     e2e_s = max(e2e_times)
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)

@@ -84,10 +84,15 @@ uint32_t brv(uint32_t x, uint32_t bits) {
   return r;
 }
 
+// Device twiddle tables for a group NTT with 2^logv words per thread. Entry layout within each
+// stage follows GroupNtt::fwd_stage / inv_stage (hb_ntt.cuh): the twiddle of block i = high*K + k
+// is stored at stage_base + k * (stage_size / K) + high.
 template <class F>
 int build_tables(hb_ctx *ctx, uint32_t logn, DevTables &t) {
   using W = typename F::W;
   const uint32_t N = 1u << logn;
+  const uint32_t logv = 4;  // every compiled group NTT holds 16 words per thread
+  const uint32_t V = 1u << logv;
   const uint64_t order = (uint64_t)F::P - 1;
   if (order % (2ull * N)) return fail(ctx, HB_ERR_UNSUPPORTED, "2N does not divide Q-1");
   W psi = 0;
@@ -95,8 +100,19 @@ int build_tables(hb_ctx *ctx, uint32_t logn, DevTables &t) {
     W c = hb::host_powmod<F>(g, order / (2ull * N));
     if (hb::host_powmod<F>(c, N) == (W)(F::P - 1)) psi = c;
   }
+  if (F::SMALL_FIRST_GEN) {
+    // Pick the primitive 2N-th root whose (2N/64)-th power is 8, so psi^(N/2) = 8^16 = 2^48 and the
+    // first forward stage on gadget digits is a shift (Goldilocks::ct_small_first).
+    const W omega = hb::host_powmod<F>(psi, 2ull * N / 64);
+    W chosen = 0;
+    for (uint32_t j = 1; j < 64 && !chosen; j += 2)
+      if (hb::host_powmod<F>(omega, j) == (W)F::SMALL_FIRST_GEN) chosen = hb::host_powmod<F>(psi, j);
+    if (!chosen || hb::host_powmod<F>(chosen, N / 2) != (W)(1ULL << 48))
+      return fail(ctx, HB_ERR_UNSUPPORTED, "no root of unity with the required power of two");
+    psi = chosen;
+  }
   const W psi_inv = hb::host_powmod<F>(psi, order - 1);
-  std::vector<W> pw(N), ipw(N), tw(N), itw(N);
+  std::vector<W> pw(N), ipw(N), tw(N, 0), itw(N, 0);
   W a = 1, b = 1;
   for (uint32_t i = 0; i < N; ++i) {
     pw[i] = a;
@@ -104,9 +120,28 @@ int build_tables(hb_ctx *ctx, uint32_t logn, DevTables &t) {
     a = hb::host_mulmod<F>(a, psi);
     b = hb::host_mulmod<F>(b, psi_inv);
   }
-  for (uint32_t k = 0; k < N; ++k) {
-    tw[k] = F::to_mont(pw[brv(k, logn)]);
-    itw[k] = F::to_mont(ipw[brv(k, logn)]);
+  for (uint32_t bb = 0; bb < logn; ++bb) {
+    // forward stage s = logn-1-bb: blocks i in [0, 2^s), twiddle psi^brv(2^s + i)
+    {
+      const uint32_t s = logn - 1 - bb;
+      const uint32_t p = (logn - 1 - bb) / logv;
+      const int lo_i = (int)logn - (int)((p + 1) * logv);
+      const uint32_t lo = lo_i > 0 ? (uint32_t)lo_i : 0;
+      const uint32_t rb = bb - lo;
+      const uint32_t K = V >> (rb + 1), highs = (1u << s) / K;
+      for (uint32_t i = 0; i < (1u << s); ++i)
+        tw[(1u << s) + (i % K) * highs + i / K] = F::to_mont(pw[brv((1u << s) + i, logn)]);
+    }
+    // inverse stage on bit bb: blocks i in [0, H), twiddle psi^-brv(H + i)
+    {
+      const uint32_t H = N >> (bb + 1);
+      const uint32_t b0 = (bb / logv) * logv;
+      const uint32_t lo = std::min(b0, logn - logv);
+      const uint32_t rb = bb - lo;
+      const uint32_t K = V >> (rb + 1), highs = H / K;
+      for (uint32_t i = 0; i < H; ++i)
+        itw[H + (i % K) * highs + i / K] = F::to_mont(ipw[brv(H + i, logn)]);
+    }
   }
   const W ninv = hb::host_powmod<F>((W)N, order - 1);
   t.n_inv = F::to_mont(ninv);

@@ -14,6 +14,10 @@
 
 #include <cstdint>
 
+#ifdef __CUDACC__
+#include "hb_gl_ptx.cuh"
+#endif
+
 #ifndef HB_HD
 #ifdef __CUDACC__
 #define HB_HD __host__ __device__ __forceinline__
@@ -86,21 +90,47 @@ struct Goldilocks {
   HB_HD static W value(W a) { return canon(a); }
   // Plain (non-Montgomery) constant: identity for Goldilocks.
   HB_HD static W to_mont(W a) { return a; }
-  // CT butterfly: (x, y) -> (x + w y, x - w y) with w canonical.
-  HB_HD static void ct(W &x, W &y, W w) {
+#ifdef __CUDA_ARCH__
+  // Device hot path: PTX carry-chain arithmetic (hb_gl_ptx.cuh).
+  // CT butterfly: (x, y) -> (x + w y, x - w y).
+  __device__ __forceinline__ static void ct(W &x, W &y, W w) {
+    const W t = glx::mul(y, w);
+    const W u = x;
+    x = glx::add_c(u, t);
+    y = glx::sub_c(u, t);
+  }
+  // GS butterfly: (x, y) -> (x + y, (x - y) w).
+  __device__ __forceinline__ static void gs(W &x, W &y, W w) {
+    const W v = glx::canon(y), u = x;
+    x = glx::add_c(u, v);
+    y = glx::mul_lazy(glx::sub_c(u, v), w);
+  }
+  // acc += x * k.
+  __device__ __forceinline__ static W mac(W acc, W x, W k) { return glx::add_c(acc, glx::mul(x, k)); }
+  // First forward stage on words below 2^15 with twiddle 2^48 (the fourth root of unity that the
+  // device tables use): x + 2^48 y and x - 2^48 y need no reduction.
+  __device__ __forceinline__ static void ct_small_first(W &x, W &y) {
+    const W t = y << 48;
+    const W u = x;
+    x = u + t;
+    y = (u + P) - t;
+  }
+#else
+  static void ct(W &x, W &y, W w) {
     const W t = mul(y, w);
     const W u = x;
     x = add_c(u, t);
     y = sub_c(u, t);
   }
-  // GS butterfly: (x, y) -> (x + y, (x - y) w).
-  HB_HD static void gs(W &x, W &y, W w) {
+  static void gs(W &x, W &y, W w) {
     const W u = x, v = y;
     x = add(u, v);
     y = mul(sub(u, v), w);
   }
-  // acc += x * k with k canonical-premultiplied key word.
-  HB_HD static W mac(W acc, W x, W k) { return add_c(acc, mul(x, k)); }
+  static W mac(W acc, W x, W k) { return add_c(acc, mul(x, k)); }
+#endif
+  // The device tables pick psi with psi^(2N/64) = 8, so psi^(N/2) = 2^48.
+  static constexpr uint64_t SMALL_FIRST_GEN = 8;
 };
 
 struct BabyBear {
@@ -142,6 +172,7 @@ struct BabyBear {
     y = mont(sub(u, v), w);
   }
   HB_HD static W mac(W acc, W x, W k) { return add(acc, mont(x, k)); }
+  static constexpr uint64_t SMALL_FIRST_GEN = 0;  // no special first stage
 };
 
 // Host-side exact helpers used to build tables.

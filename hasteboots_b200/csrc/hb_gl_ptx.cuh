@@ -1,0 +1,116 @@
+// hb_gl_ptx.cuh -- Goldilocks arithmetic written with PTX carry chains so that carries and borrows
+// come from the add/sub instructions themselves instead of 64-bit compares and selects (the
+// bootstrapping kernels are bound by the 32-bit integer ALU, where every 64-bit compare/select
+// costs several instructions). All functions accept any 64-bit word as a representative of its
+// residue mod Q = 2^64 - 2^32 + 1.
+#pragma once
+
+#include <cstdint>
+
+namespace hb {
+namespace glx {
+
+constexpr uint64_t P = 0xFFFFFFFF00000001ULL;
+
+__device__ __forceinline__ void split(uint64_t x, uint32_t &lo, uint32_t &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(x));
+}
+__device__ __forceinline__ uint64_t join(uint32_t lo, uint32_t hi) {
+  uint64_t x;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "r"(lo), "r"(hi));
+  return x;
+}
+
+// a * b folded to [0, 2^64) (not necessarily canonical).
+// Product limbs x0..x3, then x = lo + x2 2^64 + x3 2^96 = lo + x2 (2^32 - 1) - x3 (mod Q):
+//   A = x2 (2^32 - 1) + (2^32 - 1 - x3)  (fits 64 bits), r = lo + A = x + (2^32 - 1) + c 2^64,
+//   so x = r - (1 - c)(2^32 - 1) mod Q, with one more -(2^32 - 1) if that subtraction borrows.
+__device__ __forceinline__ uint64_t mul_lazy(uint64_t a, uint64_t b) {
+  uint32_t a0, a1, b0, b1;
+  split(a, a0, a1);
+  split(b, b0, b1);
+  uint32_t x0, x1, x2, x3;
+  asm("mul.lo.u32     %0, %4, %6;\n\t"
+      "mul.hi.u32     %1, %4, %6;\n\t"
+      "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
+      "madc.hi.u32    %2, %4, %7, 0;\n\t"
+      "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "madc.hi.u32    %3, %5, %7, 0;\n\t"
+      "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
+      "addc.u32       %3, %3, 0;"
+      : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  uint64_t A;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  uint32_t A0, A1;
+  split(A, A0, A1);
+  uint32_t r0, r1;
+  asm("{\n\t.reg .u32 c, m, bw;\n\t"
+      "add.cc.u32  %0, %2, %4;\n\t"
+      "addc.cc.u32 %1, %3, %5;\n\t"
+      "addc.u32    c, 0, 0;\n\t"
+      "add.u32     m, c, 0xFFFFFFFF;\n\t"  // c - 1: 0 when carried, 2^32-1 otherwise
+      "sub.cc.u32  %0, %0, m;\n\t"
+      "subc.cc.u32 %1, %1, 0;\n\t"
+      "subc.u32    bw, 0, 0;\n\t"
+      "sub.cc.u32  %0, %0, bw;\n\t"
+      "subc.u32    %1, %1, 0;\n\t}"
+      : "=&r"(r0), "=&r"(r1)
+      : "r"(x0), "r"(x1), "r"(A0), "r"(A1));
+  return join(r0, r1);
+}
+
+// Canonical representative: r >= Q exactly when r + (2^32 - 1) carries out of 64 bits.
+__device__ __forceinline__ uint64_t canon(uint64_t r) {
+  uint32_t r0, r1;
+  split(r, r0, r1);
+  uint32_t c;
+  asm("{\n\t.reg .u32 t0, t1;\n\t"
+      "add.cc.u32  t0, %1, 0xFFFFFFFF;\n\t"
+      "addc.cc.u32 t1, %2, 0;\n\t"
+      "addc.u32    %0, 0, 0;\n\t}"
+      : "=r"(c)
+      : "r"(r0), "r"(r1));
+  uint64_t out;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(out) : "r"(c), "l"(r));
+  return out;
+}
+
+__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return canon(mul_lazy(a, b)); }
+
+// a + b with b < Q: at most one carry, worth 2^32 - 1, and adding it cannot carry again.
+__device__ __forceinline__ uint64_t add_c(uint64_t a, uint64_t b) {
+  uint32_t a0, a1, b0, b1;
+  split(a, a0, a1);
+  split(b, b0, b1);
+  uint32_t s0, s1, c;
+  asm("add.cc.u32  %0, %3, %5;\n\t"
+      "addc.cc.u32 %1, %4, %6;\n\t"
+      "addc.u32    %2, 0, 0;"
+      : "=&r"(s0), "=&r"(s1), "=&r"(c)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  uint64_t out;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(out) : "r"(c), "l"(join(s0, s1)));
+  return out;
+}
+
+// a - b with b < Q: at most one borrow, worth -(2^32 - 1), and removing it cannot borrow again.
+__device__ __forceinline__ uint64_t sub_c(uint64_t a, uint64_t b) {
+  uint32_t a0, a1, b0, b1;
+  split(a, a0, a1);
+  split(b, b0, b1);
+  uint32_t d0, d1;
+  asm("{\n\t.reg .u32 bw;\n\t"
+      "sub.cc.u32  %0, %2, %4;\n\t"
+      "subc.cc.u32 %1, %3, %5;\n\t"
+      "subc.u32    bw, 0, 0;\n\t"
+      "sub.cc.u32  %0, %0, bw;\n\t"
+      "subc.u32    %1, %1, 0;\n\t}"
+      : "=&r"(d0), "=&r"(d1)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  return join(d0, d1);
+}
+
+}  // namespace glx
+}  // namespace hb

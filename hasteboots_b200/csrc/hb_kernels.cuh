@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(G * T, 1)
         if (active) {
 #pragma unroll
           for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> (j * bits)) & mask);
-          NT::forward(x, xbuf, ping, s_tw, t, sync);
+          NT::forward_small(x, xbuf, ping, s_tw, t, sync);
         }
         const W *k = pipe.acquire();
         if (active) {
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             const uint32_t sh = j * p.bits;
 #pragma unroll
             for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & br_mask);
-            NT::forward(x, xbuf, ping, s_tw, t, sync);
+            NT::forward_small(x, xbuf, ping, s_tw, t, sync);
           }
           const W *k = pipe.acquire();
           if (active) {
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
           const uint32_t sh = j * p.ks_bits;
 #pragma unroll
           for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & ks_mask);
-          NT::forward(x, xbuf, ping, s_tw, t, sync);
+          NT::forward_small(x, xbuf, ping, s_tw, t, sync);
         }
         const W *k = pipe.acquire();
         if (active) {

@@ -67,20 +67,33 @@ struct GroupNtt {
     for (int v = 0; v < V; ++v) x[v] = buf[phys(idx<LO_TO>(t, v))];
   }
 
-  // One forward (CT) stage on butterfly bit BB in a pass of layout LO.
-  template <int LO, int BB>
+  // Twiddle tables are stored stage by stage; within the 2^S entries of a stage, entry
+  // high * K + k (the k-th distinct twiddle of the threads whose bits above the pass are `high`)
+  // sits at high + k * (2^S / K), so the loads of a warp are broadcasts or consecutive words
+  // (build_tables in hb_api.cu writes this layout).
+
+  // One forward (CT) stage on butterfly bit BB in a pass of layout LO. SMALL: inputs are words
+  // below 2^15 (gadget digits) and this is the first stage, whose twiddle is 2^48.
+  template <int LO, int BB, bool SMALL>
   __device__ __forceinline__ static void fwd_stage(W (&x)[V], const W *__restrict__ tw, int t) {
     constexpr int RB = BB - LO;
     constexpr int S = LOGN - 1 - BB;
     constexpr int K = V >> (RB + 1);  // distinct twiddles per thread in this stage
-    const int base = (1 << S) + ((t >> LO) << (LOGV - RB - 1));
+    constexpr int HIGHS = (1 << S) / K;
+    if constexpr (SMALL && S == 0 && F::SMALL_FIRST_GEN != 0) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const W w = tw[base + k];
+      for (int v = 0; v < V; ++v)
+        if (!((v >> RB) & 1)) F::ct_small_first(x[v], x[v | (1 << RB)]);
+    } else {
+      const int base = (1 << S) + (t >> LO);
 #pragma unroll
-      for (int l = 0; l < (1 << RB); ++l) {
-        const int v = (k << (RB + 1)) | l;
-        F::ct(x[v], x[v | (1 << RB)], w);
+      for (int k = 0; k < K; ++k) {
+        const W w = tw[base + k * HIGHS];
+#pragma unroll
+        for (int l = 0; l < (1 << RB); ++l) {
+          const int v = (k << (RB + 1)) | l;
+          F::ct(x[v], x[v | (1 << RB)], w);
+        }
       }
     }
   }
@@ -90,10 +103,11 @@ struct GroupNtt {
     constexpr int RB = BB - LO;
     constexpr int H = N >> (BB + 1);
     constexpr int K = V >> (RB + 1);
-    const int base = H + ((t >> LO) << (LOGV - RB - 1));
+    constexpr int HIGHS = H / K;
+    const int base = H + (t >> LO);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const W w = itw[base + k];
+      const W w = itw[base + k * HIGHS];
 #pragma unroll
       for (int l = 0; l < (1 << RB); ++l) {
         const int v = (k << (RB + 1)) | l;
@@ -103,23 +117,23 @@ struct GroupNtt {
   }
 
   // Forward pass whose top butterfly bit is TOP-1; recurses to the next pass.
-  template <int TOP, int BB>
+  template <int TOP, int BB, bool SMALL>
   __device__ __forceinline__ static void fwd_stages(W (&x)[V], const W *tw, int t) {
     constexpr int LO = TOP - LOGV > 0 ? TOP - LOGV : 0;
     constexpr int LAST = TOP - LOGV > 0 ? TOP - LOGV : 0;
-    fwd_stage<LO, BB>(x, tw, t);
-    if constexpr (BB - 1 >= LAST) fwd_stages<TOP, BB - 1>(x, tw, t);
+    fwd_stage<LO, BB, SMALL>(x, tw, t);
+    if constexpr (BB - 1 >= LAST) fwd_stages<TOP, BB - 1, SMALL>(x, tw, t);
   }
-  template <int TOP>
+  template <int TOP, bool SMALL>
   __device__ __forceinline__ static void fwd_pass(W (&x)[V], W *buf, int &ping, const W *tw, int t,
                                                   const GroupSync<T> &sync) {
     constexpr int LO = TOP - LOGV > 0 ? TOP - LOGV : 0;
-    fwd_stages<TOP, TOP - 1>(x, tw, t);
+    fwd_stages<TOP, TOP - 1, SMALL>(x, tw, t);
     if constexpr (LO > 0) {
       constexpr int NEXT = LO - LOGV > 0 ? LO - LOGV : 0;
       exchange<LO, NEXT>(x, buf + ping * N, t, sync);
       ping ^= 1;
-      fwd_pass<LO>(x, buf, ping, tw, t, sync);
+      fwd_pass<LO, false>(x, buf, ping, tw, t, sync);
     }
   }
 
@@ -149,7 +163,12 @@ struct GroupNtt {
   // buf: two exchange buffers of N words (ping-pong), private to the group.
   __device__ __forceinline__ static void forward(W (&x)[V], W *buf, int &ping, const W *tw, int t,
                                                  const GroupSync<T> &sync) {
-    fwd_pass<LOGN>(x, buf, ping, tw, t, sync);
+    fwd_pass<LOGN, false>(x, buf, ping, tw, t, sync);
+  }
+  // Forward transform of a polynomial whose coefficients are below 2^15 (gadget digits).
+  __device__ __forceinline__ static void forward_small(W (&x)[V], W *buf, int &ping, const W *tw,
+                                                       int t, const GroupSync<T> &sync) {
+    fwd_pass<LOGN, true>(x, buf, ping, tw, t, sync);
   }
   // x: slots at slot_pos(t, v) -> N * (natural-order values) at natural_pos(t, v).
   __device__ __forceinline__ static void inverse(W (&x)[V], W *buf, int &ping, const W *itw, int t,
