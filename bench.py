@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=48)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--preset", type=int, default=PRESET,
+                    help="0 BABYBEAR, 1 GOLDILOCKS (default, the headline workload), 2 ZAMA")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.impl == "reference":
@@ -194,7 +196,7 @@ def main():
     from hasteboots_b200._lib import check, lib
 
     L = lib()
-    params = tfhe.Parameters.preset(PRESET)
+    params = tfhe.Parameters.preset(args.preset)
     raw = params.raw
     G = args.gates
     sk = tfhe.KeyGen.generate_secret_key(params, 0)
@@ -206,8 +208,9 @@ def main():
     c0 = sk.encrypt(bits[0], 0)
     c1 = sk.encrypt(bits[1], 1 << 20)
     width = raw.lwe_dim + 1
-    d0 = torch.from_numpy(c0.view(np.int64).copy()).cuda()
-    d1 = torch.from_numpy(c1.view(np.int64).copy()).cuda()
+    ivt = np.int64 if params.dtype == np.uint64 else np.int32
+    d0 = torch.from_numpy(c0.view(ivt).copy()).cuda()
+    d1 = torch.from_numpy(c1.view(ivt).copy()).cuda()
     dout = torch.zeros_like(d0)
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(ctx.stream_ptr())
@@ -245,13 +248,13 @@ def main():
     value = G * world / (ms_per_step / 1e3)
 
     # correctness of the timed outputs: NAND truth table on every gate
-    out = dout.cpu().numpy().view(np.uint64).reshape(G, width)
+    out = dout.cpu().numpy().view(params.dtype).reshape(G, width)
     m, noise = sk.decrypt_with_noise(out)
     ok = bool((m == 1 - (bits[0] & bits[1])).all() and (noise < params.modulus // 16).all())
 
     # end to end through the public host API (pinned buffers, copies in the timed region)
-    pin0 = torch.from_numpy(c0.view(np.int64).copy()).pin_memory()
-    pin1 = torch.from_numpy(c1.view(np.int64).copy()).pin_memory()
+    pin0 = torch.from_numpy(c0.view(ivt).copy()).pin_memory()
+    pin1 = torch.from_numpy(c1.view(ivt).copy()).pin_memory()
     pout = torch.zeros_like(pin0).pin_memory()
     e2e_times = []
     for s in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
@@ -261,14 +264,14 @@ def main():
         if s > 0:
             e2e_times.append(time.perf_counter() - a0)
     if not e2e_times:  # e2e leg disabled (profiling runs): reuse the device outputs
-        pout.copy_(torch.from_numpy(out.view(np.int64)))
+        pout.copy_(torch.from_numpy(out.view(ivt)))
         e2e_times = [float("nan")]
     e2e_s = max(e2e_times)
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_ok = bool((pout.numpy().view(np.uint64).reshape(G, width) == out).all())
+    e2e_ok = bool((pout.numpy().view(params.dtype).reshape(G, width) == out).all())
 
     # plain one-gate-per-launch form on a sample of the same gates
     P = min(args.plain_sample, G)
@@ -284,15 +287,16 @@ def main():
     pe1.synchronize()
     ctx.synchronize()
     plain_rate = P / (pe0.elapsed_time(pe1) / 1e3)
-    plain_ok = bool((pd.cpu().numpy().view(np.uint64).reshape(P, width) == out[:P]).all())
+    plain_ok = bool((pd.cpu().numpy().view(params.dtype).reshape(P, width) == out[:P]).all())
 
     # roofline: integer-pipe bound (modular multiplies), HBM shown alongside
     mm = modmuls_per_gate(raw.ring_dim, raw.lwe_dim, raw.br_len, raw.ks_len)
     modmul_launch = mm * G
     achieved = modmul_launch / (ms_per_step / 1e3)
-    bsk_bytes = raw.lwe_dim * 2 * raw.br_len * 2 * raw.ring_dim * 8
-    ksk_bytes = raw.ks_len * 2 * raw.ring_dim * 8
-    io_bytes = G * 3 * width * 8
+    ws = np.dtype(params.dtype).itemsize
+    bsk_bytes = raw.lwe_dim * 2 * raw.br_len * 2 * raw.ring_dim * ws
+    ksk_bytes = raw.ks_len * 2 * raw.ring_dim * ws
+    io_bytes = G * 3 * width * ws
     alg_bytes = bsk_bytes + ksk_bytes + io_bytes
     peaks = {}
     try:
@@ -339,7 +343,7 @@ def main():
                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "MEASURED_PEAKS.json"},
         },
         "e2e": {"value": G * world / e2e_s, "unit": "bootstraps/s",
-                "h2d_bytes_per_step": 2 * G * width * 8, "d2h_bytes_per_step": G * width * 8},
+                "h2d_bytes_per_step": 2 * G * width * ws, "d2h_bytes_per_step": G * width * ws},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "checks": {"nand_truth_table_and_noise": ok, "e2e_equals_device": e2e_ok,

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -371,12 +372,14 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
   const GateJob *djobs = (const GateJob *)ctx->jobs.ptr;
+  const unsigned grid = plain ? 1u : std::min<unsigned>(batches, (unsigned)ctx->sms);
+  prm.acc = nullptr;
+  const unsigned block = G * T;
   if (!plain) {
     prm.jobs = djobs;
     prm.njobs = (int)jobs.size();
     prm.total_batches = batches;
-    const unsigned grid = std::min<unsigned>(batches, (unsigned)ctx->sms);
-    kern<<<grid, G * T, smem, ctx->stream>>>(prm);
+    kern<<<grid, block, smem, ctx->stream>>>(prm);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
     ctx->launches += 1;
@@ -388,7 +391,7 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
     prm.njobs = 1;
     prm.total_batches = 1;
     hb::BootParams<W> one = prm;
-    kern<<<1, G * T, smem, ctx->stream>>>(one);
+    kern<<<1, block, smem, ctx->stream>>>(one);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
     ctx->launches += 1;
@@ -396,15 +399,27 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
   return HB_OK;
 }
 
-// Persistent batched form: BabyBear packs 8 gates per CTA, Goldilocks 4 (shared-memory bound).
+// Compiled gates-per-CTA variants of the persistent batched kernel (T = 64 threads per gate).
+// keys->gates_per_cta selects one (autotuned per parameter set, hb_autotune).
 int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain) {
   if (keys->p.ring_dim != 1024)
     return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
-  if (keys->p.field_id == HB_FIELD_GOLDILOCKS)
-    return plain ? launch_boot<Goldilocks, 10, 64, 1>(ctx, keys, jobs, true)
-                 : launch_boot<Goldilocks, 10, 64, 4>(ctx, keys, jobs, false);
-  return plain ? launch_boot<BabyBear, 10, 64, 1>(ctx, keys, jobs, true)
-               : launch_boot<BabyBear, 10, 64, 8>(ctx, keys, jobs, false);
+  const int G = keys->gates_per_cta;
+  if (keys->p.field_id == HB_FIELD_GOLDILOCKS) {
+    if (plain) return launch_boot<Goldilocks, 10, 64, 1>(ctx, keys, jobs, true);
+    switch (G) {
+      case 3: return launch_boot<Goldilocks, 10, 64, 3>(ctx, keys, jobs, false);
+      case 4: return launch_boot<Goldilocks, 10, 64, 4>(ctx, keys, jobs, false);
+    }
+  } else {
+    if (plain) return launch_boot<BabyBear, 10, 64, 1>(ctx, keys, jobs, true);
+    switch (G) {
+      case 4: return launch_boot<BabyBear, 10, 64, 4>(ctx, keys, jobs, false);
+      case 6: return launch_boot<BabyBear, 10, 64, 6>(ctx, keys, jobs, false);
+      case 8: return launch_boot<BabyBear, 10, 64, 8>(ctx, keys, jobs, false);
+    }
+  }
+  return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
 }
 
 template <class F>
@@ -419,6 +434,12 @@ __global__ void lwe_not_kernel(const typename F::W *in, typename F::W *out, size
 }
 
 size_t word_size(const hb_params &p) { return p.field_id == HB_FIELD_GOLDILOCKS ? 8 : 4; }
+
+int default_gates_per_cta(int field_id) {
+  const char *env = getenv("HB_GATES_PER_CTA");
+  if (env && atoi(env) > 0) return atoi(env);
+  return field_id == HB_FIELD_GOLDILOCKS ? 4 : 6;
+}
 
 }  // namespace
 
@@ -520,6 +541,7 @@ int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void 
     return e != cudaSuccess ? cuda_fail(ctx, e, "key upload") : rc;
   }
   k->bytes = (nb + nk) * ws;
+  k->gates_per_cta = default_gates_per_cta(p->field_id);
   *out = k;
   return HB_OK;
 }

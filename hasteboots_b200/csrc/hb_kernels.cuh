@@ -308,6 +308,7 @@ struct BootParams {
   const W *bsk;  // [n][2][len][2][N] slot layout, scaled (one 2N-word chunk per (i, part, j))
   const W *ksk;  // [ks_len][2][N] slot layout, scaled
   const W *tw, *itw;
+  W *acc;  // unused by this kernel (accumulators live in shared memory)
   const GateJob *jobs;
   int njobs;
   uint32_t total_batches;
@@ -419,17 +420,22 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
     }
     sync();
 
-    // ---- blind rotation (binary.rs:66-103) ----
-    W acc_x[V], acc_y[V];
+    // ---- blind rotation (binary.rs:66-103), then key switching (key_switch/rlwe.rs:115-137) ----
+    // One loop of 2n + 1 phases shares a single forward-NTT and a single inverse-NTT call site:
+    // phase 2i + part decomposes E.a (part 0) or E.b (part 1) of step i, phase 2n decomposes -acc.a
+    // for the key switch.
+    W acc_x[V], acc_y[V], e[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) acc_x[v] = acc_y[v] = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-      const int r = active ? (int)ms[i] : 0;
-      for (int part = 0; part < 2; ++part) {
-        // E = ACC * (X^r - 1) (lattice/src/rlwe.rs:437-487) in the reference's representation,
-        // then canonical for the unsigned decomposition.
-        W e[V];
-        if (active) {
+    const uint32_t phases = 2 * n + 1;
+    for (uint32_t ph = 0; ph < phases; ++ph) {
+      const bool ks = ph == 2 * n;
+      const uint32_t part = ph & 1;
+      if (active) {
+        if (!ks) {
+          // E = ACC * (X^r - 1) (lattice/src/rlwe.rs:437-487) in the reference's representation,
+          // then canonical for the unsigned decomposition.
+          const int r = (int)ms[ph >> 1];
           const W *y = part == 0 ? acc_a : acc_b;
 #pragma unroll
           for (int v = 0; v < V; ++v) {
@@ -445,53 +451,21 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             }
             e[v] = F::value(F::sub(rot, y[k]));
           }
-        }
-        for (uint32_t j = 0; j < p.len; ++j) {
-          W x[V];
-          if (active) {
-            const uint32_t sh = j * p.bits;
+        } else {
+          // sub_assign_gadget_rlwe_mul_polynomial_inplace_fast: p = -acc.a (lattice/src/rlwe.rs:1147-1166)
 #pragma unroll
-            for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & br_mask);
-            NT::forward_small(x, xbuf, ping, s_tw, t, sync);
-          }
-          const W *k = pipe.acquire();
-          if (active) {
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-              acc_x[v] = F::mac(acc_x[v], x[v], k[v * T + t]);
-              acc_y[v] = F::mac(acc_y[v], x[v], k[N + v * T + t]);
-            }
-          }
-          if (!pipe.release(src)) return;
+          for (int v = 0; v < V; ++v) e[v] = F::value(F::neg_ref(acc_a[NT::natural_pos(t, v)]));
         }
       }
-      if (active) {
-        NT::inverse(acc_x, xbuf, ping, s_itw, t, sync);
-        NT::inverse(acc_y, xbuf, ping, s_itw, t, sync);
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const int k = NT::natural_pos(t, v);
-          acc_a[k] = F::add(acc_a[k], F::canon(acc_x[v]));  // RLWE::add_assign_element_wise
-          acc_b[k] = F::add(acc_b[k], F::canon(acc_y[v]));
-          acc_x[v] = acc_y[v] = 0;
-        }
-      }
-      sync();
-    }
-
-    // ---- key switching + sample extraction (fhe_core/src/key_switch/rlwe.rs:115-137,250-286) ----
-    {
-      W e[V];
-      if (active) {
-#pragma unroll
-        for (int v = 0; v < V; ++v) e[v] = F::value(F::neg_ref(acc_a[NT::natural_pos(t, v)]));
-      }
-      for (uint32_t j = 0; j < p.ks_len; ++j) {
+      const uint32_t L = ks ? p.ks_len : p.len;
+      const uint32_t bits = ks ? p.ks_bits : p.bits;
+      const uint64_t mask = (1ULL << bits) - 1;
+      for (uint32_t j = 0; j < L; ++j) {
         W x[V];
         if (active) {
-          const uint32_t sh = j * p.ks_bits;
+          const uint32_t sh = j * bits;
 #pragma unroll
-          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & ks_mask);
+          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & mask);
           NT::forward_small(x, xbuf, ping, s_tw, t, sync);
         }
         const W *k = pipe.acquire();
@@ -504,23 +478,45 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
         }
         if (!pipe.release(src)) return;
       }
-      if (active) {
-        NT::inverse(acc_x, xbuf, ping, s_itw, t, sync);
-        NT::inverse(acc_y, xbuf, ping, s_itw, t, sync);
-        // acc.b[0] += Q >> 3 (evaluate.rs:52), then b' = b0 + INTT(...)[0]
-        const W b0 = F::canon(F::add(acc_b[0], (W)(F::P >> 3)));
-        W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
+      if (part == 0 && !ks) continue;
+      // Inverse transforms of both accumulators through one call site: h = 0 handles acc_x (the
+      // a polynomial), then acc_y moves into acc_x for h = 1 (the b polynomial).
+      W b0 = 0;
+      W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
+      if (ks && active) b0 = F::canon(F::add(acc_b[0], (W)(F::P >> 3)));  // evaluate.rs:52
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        if (active) {
+          NT::inverse(acc_x, xbuf, ping, s_itw, t, sync);
+          if (!ks) {
+            W *y = h == 0 ? acc_a : acc_b;
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const int k = NT::natural_pos(t, v);
-          const W a_k = F::canon(acc_x[v]);
-          if (k == 0) {
-            out[0] = a_k;
-            out[n] = F::canon(F::add(F::canon(acc_y[v]), b0));
-          } else if (k >= N - (int)n + 1) {
-            out[N - k] = F::neg_ref(a_k);  // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402)
+            for (int v = 0; v < V; ++v) {
+              const int k = NT::natural_pos(t, v);
+              y[k] = F::add(y[k], F::canon(acc_x[v]));  // RLWE::add_assign_element_wise
+            }
+          } else {
+            // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402): a' = [A0, -A_{N-1}, ...],
+            // b' = b0 + B0
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              const int k = NT::natural_pos(t, v);
+              const W val = F::canon(acc_x[v]);
+              if (h == 0) {
+                if (k == 0)
+                  out[0] = val;
+                else if (k >= N - (int)n + 1)
+                  out[N - k] = F::neg_ref(val);
+              } else if (k == 0) {
+                out[n] = F::canon(F::add(val, b0));
+              }
+            }
           }
-          acc_x[v] = acc_y[v] = 0;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            acc_x[v] = acc_y[v];
+            acc_y[v] = 0;
+          }
         }
       }
       sync();

@@ -35,7 +35,7 @@ struct hb_ctx {
   std::vector<std::pair<void *, size_t>> sizes;
   std::string err;
   hbrt::DevTables tables[2][13];
-  hbrt::Scratch jobs, io, mux_tmp;
+  hbrt::Scratch jobs, io, mux_tmp, acc;
   unsigned long long launches = 0;  // bootstrap kernel launches issued by this context
 };
 
@@ -44,6 +44,7 @@ struct hb_keys {
   void *bsk = nullptr;
   void *ksk = nullptr;
   size_t bytes = 0;
+  int gates_per_cta = 4;  // persistent-kernel variant (autotuned)
 };
 
 namespace hbrt {
