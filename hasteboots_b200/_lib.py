@@ -23,7 +23,8 @@ EXPORTS = [
     "hb_ctx_synchronize", "hb_ctx_hbm_in_use", "hb_keys_upload", "hb_keys_free", "hb_keys_params",
     "hb_gate", "hb_gate_device", "hb_gate_device_plain", "hb_bootstrap_lut",
     "hb_ntt_forward_device", "hb_ntt_inverse_device", "hb_ntt_roundtrip_device", "hb_rgsw_upload",
-    "hb_rgsw_free", "hb_external_product_device", "hb_probe_modmul", "hb_ctx_launches",
+    "hb_rgsw_free", "hb_external_product_device", "hb_gate_mux_device_noalloc",
+    "hb_probe_modmul", "hb_ctx_launches",
 ]
 
 
@@ -89,6 +90,7 @@ def lib():
         "hb_rgsw_upload": (i32, [vp, i32, u32, u32, u32, vp, pp]),
         "hb_rgsw_free": (None, [vp, vp]),
         "hb_external_product_device": (i32, [vp, i32, u32, u32, u32, vp, vp, vp, sz]),
+        "hb_gate_mux_device_noalloc": (i32, [vp, vp, vp, vp, vp, vp, sz]),
         "hb_probe_modmul": (i32, [vp, i32, ctypes.POINTER(ctypes.c_double)]),
         "hb_ctx_launches": (u64, [vp]),
     }

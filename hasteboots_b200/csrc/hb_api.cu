@@ -785,3 +785,145 @@ int hb_probe_modmul(hb_ctx *ctx, int field_id, double *modmul_per_s) {
 uint64_t hb_ctx_launches(const hb_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free MUX (hb_gate_mux_device_noalloc)
+//
+// For callers that may not allocate device memory during a call. Everything the two-layer MUX
+// needs beyond its inputs and outputs -- the status word, the job table and the two intermediate
+// ciphertext batches -- lives in one array compiled into this library.
+// ------------------------------------------------------------------------------------------
+
+namespace {
+
+constexpr size_t kNoAllocBytes = 16u << 20;  // 16 MiB, held by every GPU that loads the library
+constexpr size_t kNoAllocStatus = 0;         // int status word
+constexpr size_t kNoAllocJobs = 256;         // three GateJob records
+constexpr size_t kNoAllocData = 1024;        // t0 | t1, count * (n + 1) words each
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[256] = {};  // device address of g_noalloc_scratch, per device
+
+// Host code only sees a host-side stand-in named g_noalloc_scratch; the kernels need the device
+// address, looked up once per device with that device current.
+int noalloc_address(hb_ctx *ctx, unsigned char **out) {
+  if (ctx->device < 0 || ctx->device >= 256) return fail(ctx, HB_ERR_INVALID, "device id out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[ctx->device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(no-allocation scratch)");
+    g_noalloc_addr[ctx->device] = p;
+  }
+  *out = (unsigned char *)g_noalloc_addr[ctx->device];
+  return HB_OK;
+}
+
+template <class F, int LOGN, int T, int G>
+int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJob *djobs, int njobs,
+                   uint32_t batches, int *dstatus) {
+  using W = typename F::W;
+  constexpr int N = 1 << LOGN;
+  hb::BootParams<W> prm{};
+  prm.bsk = (const W *)keys->bsk;
+  prm.ksk = (const W *)keys->ksk;
+  prm.tw = (const W *)tb->tw;
+  prm.itw = (const W *)tb->itw;
+  prm.acc = nullptr;
+  prm.jobs = djobs;
+  prm.njobs = njobs;
+  prm.total_batches = batches;
+  prm.n = keys->p.lwe_dim;
+  prm.len = keys->p.br_len;
+  prm.bits = keys->p.br_bits;
+  prm.ks_len = keys->p.ks_len;
+  prm.ks_bits = keys->p.ks_bits;
+  prm.status = dstatus;
+  prm.budget = wait_budget();
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, kStages>;
+  const size_t smem = hb::boot_smem_bytes<W, N, G, kStages>(prm.n);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
+  const unsigned grid = std::min<unsigned>(batches, (unsigned)ctx->sms);
+  kern<<<grid, G * T, smem, ctx->stream>>>(prm);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? HB_OK : cuda_fail(ctx, e, "bootstrap launch");
+}
+
+int noalloc_layer(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJob *djobs, int njobs,
+                  uint32_t batches, int *dstatus) {
+  const int G = keys->gates_per_cta;
+  if (keys->p.field_id == HB_FIELD_GOLDILOCKS) {
+    if (G == 3) return launch_noalloc<Goldilocks, 10, 64, 3>(ctx, keys, tb, djobs, njobs, batches, dstatus);
+    if (G == 4) return launch_noalloc<Goldilocks, 10, 64, 4>(ctx, keys, tb, djobs, njobs, batches, dstatus);
+  } else {
+    if (G == 4) return launch_noalloc<BabyBear, 10, 64, 4>(ctx, keys, tb, djobs, njobs, batches, dstatus);
+    if (G == 6) return launch_noalloc<BabyBear, 10, 64, 6>(ctx, keys, tb, djobs, njobs, batches, dstatus);
+    if (G == 8) return launch_noalloc<BabyBear, 10, 64, 8>(ctx, keys, tb, djobs, njobs, batches, dstatus);
+  }
+  return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
+}
+
+}  // namespace
+
+extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void *c0, const void *c1,
+                                          const void *c2, void *out, size_t count) {
+  if (!ctx || !keys) return HB_ERR_INVALID;
+  if (!c0 || !c1 || !c2 || !out) return fail(ctx, HB_ERR_INVALID, "missing ciphertext buffer");
+  if (count == 0) return HB_OK;
+  const hb_params &p = keys->p;
+  if (p.ring_dim != 1024) return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
+  const bool gl = p.field_id == HB_FIELD_GOLDILOCKS;
+  const size_t width = (size_t)p.lwe_dim + 1, ws = gl ? 8 : 4;
+  const size_t max_gates = (kNoAllocBytes - kNoAllocData) / (2 * width * ws);
+  if (count > max_gates)
+    return fail(ctx, HB_ERR_INVALID,
+                "%zu gates exceed the no-allocation scratch of %zu bytes (at most %zu gates for this "
+                "parameter set)", count, kNoAllocBytes, max_gates);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  // The NTT tables were built when the keys were uploaded; this path must not build (allocate) them.
+  const DevTables *tb = &ctx->tables[p.field_id][10];
+  if (!tb->tw) return fail(ctx, HB_ERR_INVALID, "keys were not uploaded on this context");
+  unsigned char *base = nullptr;
+  int rc = noalloc_address(ctx, &base);
+  if (rc) return rc;
+  int *dstatus = (int *)(base + kNoAllocStatus);
+  GateJob *djobs = (GateJob *)(base + kNoAllocJobs);
+  unsigned char *t0 = base + kNoAllocData, *t1 = t0 + count * width * ws;
+
+  // MUX (tfhe/src/bfhe/evaluate.rs:245-262): t0 = and(c0, c1), t1 = and(not c0, c2) in one launch,
+  // then out = bootstrap(t0 + t1, or) in a second.
+  const int G = keys->gates_per_cta;
+  GateJob jobs[3];
+  jobs[0] = gl ? make_job<Goldilocks>(HB_GATE_AND, p.ring_dim, c0, c1, nullptr, t0, (uint32_t)count)
+               : make_job<BabyBear>(HB_GATE_AND, p.ring_dim, c0, c1, nullptr, t0, (uint32_t)count);
+  jobs[1] = jobs[0];
+  jobs[1].in1 = c2;
+  jobs[1].out = t1;
+  jobs[1].s0 = -1;  // not(c0) = -c0 + Q/4 on the body
+  jobs[1].add_b = gl ? (Goldilocks::P >> 2) : (BabyBear::P >> 2);
+  jobs[2] = gl ? make_job<Goldilocks>(HB_GATE_MUX, p.ring_dim, t0, t1, nullptr, out, (uint32_t)count)
+               : make_job<BabyBear>(HB_GATE_MUX, p.ring_dim, t0, t1, nullptr, out, (uint32_t)count);
+  const uint32_t per_job = (uint32_t)((count + G - 1) / G);
+  jobs[0].first_batch = 0;
+  jobs[1].first_batch = per_job;
+  jobs[2].first_batch = 0;
+
+  // The array keeps the previous call's contents: the status word must start at zero.
+  e = cudaMemsetAsync(dstatus, 0, sizeof(int), ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(djobs, jobs, sizeof(jobs), cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "no-allocation scratch setup");
+  rc = noalloc_layer(ctx, keys, tb, djobs, 2, 2 * per_job, dstatus);
+  if (!rc) rc = noalloc_layer(ctx, keys, tb, djobs + 2, 1, per_job, dstatus);
+  if (rc) return rc;
+  int h = 0;
+  e = cudaMemcpyAsync(&h, dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "no-allocation MUX");
+  if (h) return fail(ctx, HB_ERR_TIMEOUT, "a device-side wait exceeded its limit (status %d)", h);
+  return HB_OK;
+}

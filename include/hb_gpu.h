@@ -165,6 +165,21 @@ int hb_external_product_device(hb_ctx *ctx, int field_id, uint32_t log_n, uint32
                                uint32_t len, const void *d_rgsw, const void *rlwe_in,
                                void *rlwe_out, size_t count);
 
+/* Evaluator::mux for callers that cannot allocate device memory during a call: a serving process
+ * that reserves its whole HBM budget at start-up and may not take a cudaMalloc on its request path
+ * (cudaMalloc can synchronise the device and fragments the heap), or a host that hands out all
+ * device memory from its own pool. No counterpart in the reference.
+ * The intermediate ciphertexts, job table and status word live in a 16 MiB array compiled into the
+ * library, which every GPU that loads the library holds until the process exits. count is at most
+ * (16 MiB - 1 KiB) / (2 (n + 1) word bytes): 1438 gates for the Goldilocks sets, 2876 for BabyBear;
+ * larger counts return HB_ERR_INVALID. The first call on a device looks up the array's device
+ * address, so make that call before any stream capture. Every call uses the same array: calls whose
+ * work overlaps on the GPU (other streams, contexts or host threads) race and must be serialised.
+ * Device pointers in; returns when `out` holds the result (synchronises the context stream).
+ * The keys must have been uploaded on this context. */
+int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void *c0, const void *c1,
+                               const void *c2, void *out, size_t count);
+
 /* ---- diagnostics ------------------------------------------------------------------------ */
 
 /* Field-multiplication throughput of this device (independent register chains, all SMs): the
