@@ -166,6 +166,176 @@ def run_reference(args, rank, world):
     return 0
 
 
+def _timed(stream, fn, reps):
+    """Device time of `reps` calls of fn() enqueued on `stream` (CUDA events), in ms."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def workload_mixed(args):
+    """64 jobs, gate counts log-uniform in [1, 4096] (seed 4), parameter set drawn uniformly from
+    {ZAMA, GOLDILOCKS, BABYBEAR}, random input bits, gate kinds cycling NAND..MAJORITY; one CUDA graph
+    per step holding one persistent launch per set, SMs split by autotuned per-set throughput."""
+    import torch
+    from hasteboots_b200 import tfhe
+    from hasteboots_b200._lib import lib
+    ctx = tfhe.Context(0)
+    evs = {}
+    for pid in (0, 1, 2):
+        sk = tfhe.KeyGen.generate_secret_key(tfhe.Parameters.preset(pid), 0)
+        evs[pid] = (sk, tfhe.Evaluator(sk, ctx))
+    tuned = {pid: tfhe.autotune(ev)[:2] for pid, (sk, ev) in evs.items()}
+    rng = np.random.default_rng(4)
+    names = ["nand", "and", "or", "nor", "xor", "xnor", "majority"]
+    jobs, checks = [], []
+    for i in range(64):
+        pid = int(rng.integers(0, 3))
+        count = int(np.clip(np.round(np.exp(rng.uniform(0, np.log(4096)))), 1, 4096))
+        gate = names[i % len(names)]
+        sk, ev = evs[pid]
+        bits = rng.integers(0, 2, (3, count)).astype(np.uint8)
+        ivt = np.int64 if sk.params.dtype == np.uint64 else np.int32
+        cs = [torch.from_numpy(sk.encrypt(bits[k], (i << 24) + (k << 20)).view(ivt)).cuda() for k in range(3)]
+        out = torch.zeros_like(cs[0])
+        jobs.append((ev, gate, cs[0], cs[1], cs[2] if gate == "majority" else None, out))
+        a, b, c = bits
+        checks.append((sk, out, {"nand": 1 - (a & b), "and": a & b, "or": a | b, "nor": 1 - (a | b),
+                                 "xor": a ^ b, "xnor": 1 - (a ^ b),
+                                 "majority": (a & b) | (b & c) | (a & c)}[gate]))
+    torch.cuda.synchronize()
+    batch = tfhe.Batch(ctx, jobs)
+    info = batch.info()
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    for _ in range(args.warmup):
+        batch.launch()
+    ctx.synchronize()
+    l0 = lib().hb_ctx_launches(ctx.handle)
+    with ClockSampler(physical_gpu_index(0)) as clk:
+        ms = _timed(stream, batch.launch, args.steps)
+    ctx.synchronize()
+    launches = lib().hb_ctx_launches(ctx.handle) - l0
+    ok = all((sk.decrypt(out.cpu().numpy().view(sk.params.dtype)) == exp).all() for sk, out, exp in checks)
+    per = ms / args.steps
+    line = {"metric": "mixed-set batched bootstraps/s (one graph launch per step)",
+            "value": info["gates"] / (per / 1e3), "unit": "bootstraps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per, "higher_is_better": True,
+            "dtype": "u64+u32", "data": "synthetic (seed-0 keys, seed-4 job plan and bits)",
+            "config": {"workload": "64 jobs, log-uniform 1-4096 gates, sets uniform over ZAMA/GOLDILOCKS/BABYBEAR",
+                       "gates": info["gates"], "kernels_per_graph": info["launches"],
+                       "sm_split": info["sm_split"],
+                       "autotuned_gates_per_cta": {str(k): v[0] for k, v in tuned.items()},
+                       "autotuned_gates_per_s": {str(k): v[1] for k, v in tuned.items()}},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "checks": {"truth_tables": bool(ok)}}
+    print(json.dumps(line), flush=True)
+    batch.free()
+    for sk, ev in evs.values():
+        ev.keys.free()
+    ctx.close()
+    return 0 if ok else 1
+
+
+def workload_ntt(args):
+    """Kernel microbench: batched negacyclic NTT->INTT round trip and one RLWE x RGSW external
+    product over Goldilocks, N in {1024, 2048}, 4096 polynomials (round trip) / 4096 RLWEs (product),
+    coefficients uniform in [0, Q) (seed 1), RGSW l = 13 rows at B = 2^5 uniform (seed 2)."""
+    import torch
+    from hasteboots_b200 import tfhe
+    from hasteboots_b200._lib import check, lib
+    ctx = tfhe.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    Q = 0xFFFFFFFF00000001
+    res = {}
+    probe = ctypes.c_double()
+    check(lib().hb_probe_modmul(ctx.handle, 1, ctypes.byref(probe)), "probe", ctx.handle)
+    for log_n in (10, 11):
+        n = 1 << log_n
+        x = (np.random.default_rng(1).integers(0, 2**63, (4096, n), dtype=np.uint64) * 2) % np.uint64(Q)
+        dx = torch.from_numpy(x.view(np.int64)).cuda()
+        dy = torch.zeros_like(dx)
+        torch.cuda.synchronize()
+        rt = lambda: check(lib().hb_ntt_roundtrip_device(ctx.handle, 1, log_n, dx.data_ptr(), dy.data_ptr(), 4096), "rt")
+        for _ in range(args.warmup):
+            rt()
+        ms = _timed(stream, rt, args.steps) / args.steps
+        ok = bool((dy.cpu().numpy().view(np.uint64) == x).all())
+        mm = 2 * 4096 * (n // 2) * log_n
+        res[f"roundtrip_N{n}"] = {"ms": ms, "polys_per_s": 4096 / (ms / 1e3),
+                                 "gmodmul_per_s": mm / (ms / 1e3) / 1e9,
+                                 "frac_of_modmul_probe": mm / (ms / 1e3) / probe.value,
+                                 "hbm_gbs": 2 * 4096 * n * 8 / (ms / 1e3) / 1e9, "exact": ok}
+        length, bits = 13, 5
+        rgsw = np.random.default_rng(2).integers(0, 2**63, 2 * length * 2 * n, dtype=np.uint64) % np.uint64(Q)
+        h = ctypes.c_void_p()
+        check(lib().hb_rgsw_upload(ctx.handle, 1, log_n, bits, length, rgsw.ctypes.data_as(ctypes.c_void_p),
+                                   ctypes.byref(h)), "rgsw", ctx.handle)
+        rl = torch.from_numpy((np.random.default_rng(1).integers(0, 2**63, (4096, 2 * n), dtype=np.uint64)
+                               % np.uint64(Q)).view(np.int64)).cuda()
+        ro = torch.zeros_like(rl)
+        torch.cuda.synchronize()
+        ep = lambda: check(lib().hb_external_product_device(ctx.handle, 1, log_n, bits, length, h, rl.data_ptr(),
+                                                            ro.data_ptr(), 4096), "ext")
+        for _ in range(args.warmup):
+            ep()
+        ms = _timed(stream, ep, args.steps) / args.steps
+        mm = 4096 * ((2 * length + 2) * (n // 2) * log_n + 4 * length * n)
+        res[f"ext_product_N{n}"] = {"ms": ms, "products_per_s": 4096 / (ms / 1e3),
+                                   "gmodmul_per_s": mm / (ms / 1e3) / 1e9,
+                                   "frac_of_modmul_probe": mm / (ms / 1e3) / probe.value}
+        lib().hb_rgsw_free(ctx.handle, h)
+    line = {"metric": "NTT round trip and RLWE x RGSW external product throughput (Goldilocks)",
+            "value": res["ext_product_N1024"]["products_per_s"], "unit": "external products/s (N=1024)",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "u64", "data": "synthetic (seeds 1, 2)", "modmul_probe_g_per_s": probe.value / 1e9,
+            "config": {"workload": "4096 polynomials / 4096 RLWEs per launch, N in {1024, 2048}, RGSW l=13 B=2^5"},
+            "results": res}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0 if all(v.get("exact", True) for v in res.values()) else 1
+
+
+def workload_serve(args):
+    raise SystemExit("serve workload: request loop not built yet")
+
+
+def workload_single(args):
+    """One BabyBear NAND gate, one launch (config 1): latency of the plain form."""
+    import torch
+    from hasteboots_b200 import tfhe
+    from hasteboots_b200._lib import check, lib
+    sk = tfhe.KeyGen.generate_secret_key(tfhe.Parameters.preset(0), 0)
+    ctx = tfhe.Context(0)
+    ev = tfhe.Evaluator(sk, ctx)
+    c0, c1 = sk.encrypt([1], 0), sk.encrypt([1], 1)
+    d0 = torch.from_numpy(c0.view(np.int32).copy()).cuda()
+    d1 = torch.from_numpy(c1.view(np.int32).copy()).cuda()
+    do = torch.zeros_like(d0)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    one = lambda: check(lib().hb_gate_device_plain(ctx.handle, ev.keys.handle, 0, d0.data_ptr(), d1.data_ptr(),
+                                                   do.data_ptr(), 1), "plain", ctx.handle)
+    for _ in range(args.warmup):
+        one()
+    times = [_timed(stream, one, 1) for _ in range(args.steps)]
+    bit = sk.decrypt(do.cpu().numpy().view(np.uint32))[0]
+    line = {"metric": "single NAND bootstrap latency, BABYBEAR_BINARY_128_BITS", "value": float(np.median(times)),
+            "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "dtype": "u32", "data": "synthetic (seed-0 keys)",
+            "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
+            "config": {"workload": "1 NAND gate, one kernel launch (one 64-thread group)"},
+            "checks": {"nand(1,1)=0": bool(bit == 0)}}
+    print(json.dumps(line), flush=True)
+    ev.keys.free()
+    ctx.close()
+    return 0 if bit == 0 else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -178,10 +348,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preset", type=int, default=PRESET,
                     help="0 BABYBEAR, 1 GOLDILOCKS (default, the headline workload), 2 ZAMA")
+    ap.add_argument("--workload", default="gates", choices=["gates", "mixed", "ntt", "single", "serve"],
+                    help="gates: 16384 NAND gates (default, the contract line); mixed: 64 jobs across "
+                         "the three sets in one graph; ntt: NTT/external-product microbench; single: "
+                         "one BabyBear NAND; serve: the request loop")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: mean requests per second")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != "gates":
+        import torch
+        torch.cuda.set_device(local_rank)
+        fn = {"mixed": workload_mixed, "ntt": workload_ntt, "single": workload_single,
+              "serve": workload_serve}[args.workload]
+        return fn(args) if rank == 0 else 0
 
     import torch
     import torch.distributed as dist
@@ -219,6 +401,7 @@ def main():
         check(L.hb_gate_device(ctx.handle, ev.keys.handle, GATE_NAND, d0.data_ptr(), d1.data_ptr(),
                                None, dout.data_ptr(), G), "hb_gate_device", ctx.handle)
 
+    tuned_g, tuned_rate, tuned_cached = tfhe.autotune(ev)  # setup, outside the timed region
     # roofline denominator: measured field-multiplication throughput of this GPU
     probe = ctypes.c_double()
     check(L.hb_probe_modmul(ctx.handle, raw.field_id, ctypes.byref(probe)), "probe", ctx.handle)
@@ -324,6 +507,8 @@ def main():
             "gates_per_gpu": G,
             "parallelism": f"replicas x{world}",
             "l2": "inputs (191 MB) and BSK (191 MB) exceed L2; no flush",
+            "gates_per_cta": tuned_g,
+            "autotune": {"gates_per_s_sample": tuned_rate, "from_cache": tuned_cached},
         },
         "latency_ms": {"p50": ms_per_step, "p99": ms_per_step,
                        "note": "every gate of a batched launch completes with the launch"},

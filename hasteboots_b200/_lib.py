@@ -23,7 +23,9 @@ EXPORTS = [
     "hb_ctx_synchronize", "hb_ctx_hbm_in_use", "hb_keys_upload", "hb_keys_free", "hb_keys_params",
     "hb_gate", "hb_gate_device", "hb_gate_device_plain", "hb_bootstrap_lut",
     "hb_ntt_forward_device", "hb_ntt_inverse_device", "hb_ntt_roundtrip_device", "hb_rgsw_upload",
-    "hb_rgsw_free", "hb_external_product_device", "hb_gate_mux_device_noalloc",
+    "hb_rgsw_free", "hb_external_product_device", "hb_autotune", "hb_keys_set_gates_per_cta",
+    "hb_keys_gates_per_cta", "hb_batch_create", "hb_batch_launch", "hb_batch_free",
+    "hb_batch_info", "hb_gate_mux_device_noalloc",
     "hb_probe_modmul", "hb_ctx_launches",
 ]
 
@@ -41,6 +43,18 @@ class HbParams(ctypes.Structure):
         ("lwe_noise_std", ctypes.c_double),
         ("ring_noise_std", ctypes.c_double),
         ("ks_noise_std", ctypes.c_double),
+    ]
+
+
+class HbJob(ctypes.Structure):
+    _fields_ = [
+        ("keys", ctypes.c_void_p),
+        ("gate", ctypes.c_int32),
+        ("count", ctypes.c_uint32),
+        ("c0", ctypes.c_void_p),
+        ("c1", ctypes.c_void_p),
+        ("c2", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
     ]
 
 
@@ -90,6 +104,13 @@ def lib():
         "hb_rgsw_upload": (i32, [vp, i32, u32, u32, u32, vp, pp]),
         "hb_rgsw_free": (None, [vp, vp]),
         "hb_external_product_device": (i32, [vp, i32, u32, u32, u32, vp, vp, vp, sz]),
+        "hb_autotune": (i32, [vp, vp, u32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]),
+        "hb_keys_set_gates_per_cta": (i32, [vp, i32]),
+        "hb_keys_gates_per_cta": (i32, [vp]),
+        "hb_batch_create": (i32, [vp, ctypes.POINTER(HbJob), sz, pp]),
+        "hb_batch_launch": (i32, [vp, vp]),
+        "hb_batch_free": (None, [vp, vp]),
+        "hb_batch_info": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(i32), ctypes.POINTER(i32), i32]),
         "hb_gate_mux_device_noalloc": (i32, [vp, vp, vp, vp, vp, vp, sz]),
         "hb_probe_modmul": (i32, [vp, i32, ctypes.POINTER(ctypes.c_double)]),
         "hb_ctx_launches": (u64, [vp]),

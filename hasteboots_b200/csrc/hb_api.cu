@@ -422,6 +422,70 @@ int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain)
   return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
 }
 
+// Gates-per-CTA variants compiled for each field (the autotuner's candidates).
+const std::vector<int> &variants(int field_id) {
+  static const std::vector<int> gl = {3, 4}, bb = {4, 6, 8};
+  return field_id == HB_FIELD_GOLDILOCKS ? gl : bb;
+}
+
+uint32_t batches_of(const std::vector<GateJob> &jobs, int G) {
+  uint32_t b = 0;
+  for (auto &j : jobs) b += (j.count + G - 1) / G;
+  return b;
+}
+
+// One batched persistent launch over a device job table that is already in place.
+template <class F, int LOGN, int T, int G>
+int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, uint32_t batches,
+                 unsigned grid, cudaStream_t stream) {
+  using W = typename F::W;
+  constexpr int N = 1 << LOGN;
+  DevTables *tb;
+  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb);
+  if (rc) return rc;
+  hb::BootParams<W> prm{};
+  prm.bsk = (const W *)keys->bsk;
+  prm.ksk = (const W *)keys->ksk;
+  prm.tw = (const W *)tb->tw;
+  prm.itw = (const W *)tb->itw;
+  prm.acc = nullptr;
+  prm.jobs = djobs;
+  prm.njobs = njobs;
+  prm.total_batches = batches;
+  prm.n = keys->p.lwe_dim;
+  prm.len = keys->p.br_len;
+  prm.bits = keys->p.br_bits;
+  prm.ks_len = keys->p.ks_len;
+  prm.ks_bits = keys->p.ks_bits;
+  prm.status = ctx->d_status;
+  prm.budget = wait_budget();
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, kStages>;
+  const size_t smem = hb::boot_smem_bytes<W, N, G, kStages>(prm.n);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
+  grid = std::max(1u, std::min(grid, batches));
+  kern<<<grid, G * T, smem, stream>>>(prm);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
+  ctx->launches += 1;
+  return HB_OK;
+}
+
+int launch_table_any(hb_ctx *ctx, hb_keys *keys, int G, const GateJob *djobs, int njobs,
+                     uint32_t batches, unsigned grid, cudaStream_t stream) {
+  if (keys->p.field_id == HB_FIELD_GOLDILOCKS) {
+    if (G == 3) return launch_table<Goldilocks, 10, 64, 3>(ctx, keys, djobs, njobs, batches, grid, stream);
+    if (G == 4) return launch_table<Goldilocks, 10, 64, 4>(ctx, keys, djobs, njobs, batches, grid, stream);
+  } else {
+    if (G == 4) return launch_table<BabyBear, 10, 64, 4>(ctx, keys, djobs, njobs, batches, grid, stream);
+    if (G == 6) return launch_table<BabyBear, 10, 64, 6>(ctx, keys, djobs, njobs, batches, grid, stream);
+    if (G == 8) return launch_table<BabyBear, 10, 64, 8>(ctx, keys, djobs, njobs, batches, grid, stream);
+  }
+  return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
+}
+
+bool single_bootstrap_gate(int gate) { return gate >= HB_GATE_NAND && gate <= HB_GATE_MAJORITY; }
+
 template <class F>
 __global__ void lwe_not_kernel(const typename F::W *in, typename F::W *out, size_t words,
                                uint32_t width) {
@@ -927,3 +991,231 @@ extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void
   if (h) return fail(ctx, HB_ERR_TIMEOUT, "a device-side wait exceeded its limit (status %d)", h);
   return HB_OK;
 }
+
+// ------------------------------------------------------------------------------------------
+// Autotuner and mixed-set batches
+// ------------------------------------------------------------------------------------------
+
+extern "C" int hb_keys_set_gates_per_cta(hb_keys *keys, int gates_per_cta) {
+  if (!keys) return HB_ERR_INVALID;
+  for (int g : variants(keys->p.field_id))
+    if (g == gates_per_cta) {
+      keys->gates_per_cta = g;
+      return HB_OK;
+    }
+  return HB_ERR_UNSUPPORTED;
+}
+
+extern "C" int hb_keys_gates_per_cta(const hb_keys *keys) { return keys ? keys->gates_per_cta : 0; }
+
+extern "C" int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, int *chosen,
+                           double *gates_per_s) {
+  if (!ctx || !keys) return HB_ERR_INVALID;
+  if (keys->p.ring_dim != 1024) return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
+  cudaSetDevice(ctx->device);
+  if (sample_gates == 0) sample_gates = (uint32_t)ctx->sms * 24;  // whole waves for every candidate G
+  const size_t width = (size_t)keys->p.lwe_dim + 1, ws = word_size(keys->p);
+  const size_t bytes = (size_t)sample_gates * width * ws;
+  void *buf = nullptr, *tab = nullptr;
+  int rc = dev_alloc(ctx, 2 * bytes, &buf);
+  if (!rc) rc = dev_alloc(ctx, sizeof(GateJob), &tab);
+  if (rc) {
+    dev_free(ctx, buf);
+    return rc;
+  }
+  cudaMemsetAsync(buf, 0, 2 * bytes, ctx->stream);  // any ciphertexts time the same: zeros
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best_g = keys->gates_per_cta;
+  double best_rate = 0;
+  for (int G : variants(keys->p.field_id)) {
+    std::vector<GateJob> jobs{keys->p.field_id == HB_FIELD_GOLDILOCKS
+                                  ? make_job<Goldilocks>(HB_GATE_NAND, 1024, buf, buf, nullptr,
+                                                         (char *)buf + bytes, sample_gates)
+                                  : make_job<BabyBear>(HB_GATE_NAND, 1024, buf, buf, nullptr,
+                                                       (char *)buf + bytes, sample_gates)};
+    jobs[0].first_batch = 0;
+    const uint32_t batches = batches_of(jobs, G);
+    cudaMemcpyAsync(tab, jobs.data(), sizeof(GateJob), cudaMemcpyHostToDevice, ctx->stream);
+    float best_ms = 1e30f;
+    for (int rep = 0; rep < 3 && !rc; ++rep) {  // rep 0 warms up
+      cudaEventRecord(e0, ctx->stream);
+      rc = launch_table_any(ctx, keys, G, (const GateJob *)tab, 1, batches, ctx->sms, ctx->stream);
+      cudaEventRecord(e1, ctx->stream);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(ctx, cudaGetLastError(), "autotune");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) best_ms = std::min(best_ms, ms);
+    }
+    if (rc) break;
+    const double rate = sample_gates / (best_ms * 1e-3);
+    if (rate > best_rate) {
+      best_rate = rate;
+      best_g = G;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dev_free(ctx, buf);
+  dev_free(ctx, tab);
+  if (!rc) rc = check_status(ctx);
+  if (rc) return rc;
+  keys->gates_per_cta = best_g;
+  keys->gates_per_s = best_rate;
+  if (chosen) *chosen = best_g;
+  if (gates_per_s) *gates_per_s = best_rate;
+  return HB_OK;
+}
+
+struct hb_batch {
+  struct Group {
+    hb_keys *keys = nullptr;
+    void *djobs = nullptr;
+    int njobs = 0;
+    uint32_t batches = 0;
+    unsigned grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+  };
+  std::vector<Group> groups;
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t gates = 0;
+};
+
+extern "C" void hb_batch_free(hb_ctx *ctx, hb_batch *b) {
+  if (!ctx || !b) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto &g : b->groups) {
+    dev_free(ctx, g.djobs);
+    if (g.stream) cudaStreamDestroy(g.stream);
+    if (g.done) cudaEventDestroy(g.done);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  delete b;
+}
+
+extern "C" int hb_batch_create(hb_ctx *ctx, const hb_job *jobs, size_t njobs, hb_batch **out) {
+  if (!ctx || !out || (njobs && !jobs)) return HB_ERR_INVALID;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  // group the jobs by key set: one persistent launch per parameter set
+  std::vector<hb_keys *> keysets;
+  std::vector<std::vector<GateJob>> tables_h;
+  uint64_t gates = 0;
+  for (size_t i = 0; i < njobs; ++i) {
+    const hb_job &j = jobs[i];
+    if (!j.keys || !j.c0 || !j.out || !single_bootstrap_gate(j.gate) || (j.count && !j.c1) ||
+        (j.gate == HB_GATE_MAJORITY && !j.c2))
+      return fail(ctx, HB_ERR_INVALID, "job %zu: bad keys, buffers or gate (batches take single-bootstrap gates)", i);
+    if (j.keys->p.ring_dim != 1024) return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
+    if (j.count == 0) continue;
+    size_t k = 0;
+    while (k < keysets.size() && keysets[k] != j.keys) ++k;
+    if (k == keysets.size()) {
+      keysets.push_back(j.keys);
+      tables_h.emplace_back();
+    }
+    const bool gl = j.keys->p.field_id == HB_FIELD_GOLDILOCKS;
+    tables_h[k].push_back(gl ? make_job<Goldilocks>(j.gate, 1024, j.c0, j.c1, j.c2, j.out, j.count)
+                             : make_job<BabyBear>(j.gate, 1024, j.c0, j.c1, j.c2, j.out, j.count));
+    gates += j.count;
+  }
+  hb_batch *b = new hb_batch();
+  b->gates = gates;
+  // SM partition by estimated work: gates / measured (or default) per-set throughput
+  std::vector<double> work(keysets.size());
+  double total = 0;
+  for (size_t k = 0; k < keysets.size(); ++k) {
+    double g = 0;
+    for (auto &t : tables_h[k]) g += t.count;
+    const hb_keys *ks = keysets[k];
+    double rate = ks->gates_per_s;
+    if (rate <= 0) {  // uncalibrated: scale by modular multiplies per gate, BabyBear ~4x cheaper each
+      const double logn = 10, N = 1024;
+      const double mm = ks->p.lwe_dim * ((2.0 * ks->p.br_len + 2) * N / 2 * logn + 4.0 * ks->p.br_len * N);
+      rate = 1e12 / mm * (ks->p.field_id == HB_FIELD_GOLDILOCKS ? 1.0 : 4.0);
+    }
+    work[k] = g / rate;
+    total += work[k];
+  }
+  int rc = HB_OK;
+  unsigned used = 0;
+  for (size_t k = 0; k < keysets.size() && !rc; ++k) {
+    hb_batch::Group grp;
+    grp.keys = keysets[k];
+    const int G = grp.keys->gates_per_cta;
+    auto &tab = tables_h[k];
+    uint32_t bsum = 0;
+    for (auto &t : tab) {
+      t.first_batch = bsum;
+      bsum += (t.count + G - 1) / G;
+    }
+    grp.batches = bsum;
+    grp.njobs = (int)tab.size();
+    unsigned share = (unsigned)std::lround(ctx->sms * work[k] / total);
+    if (k + 1 == keysets.size()) share = (unsigned)ctx->sms > used ? ctx->sms - used : 1;
+    grp.grid = std::max(1u, std::min(share, bsum));
+    used += grp.grid;
+    rc = dev_alloc(ctx, sizeof(GateJob) * tab.size(), &grp.djobs);
+    if (!rc) {
+      cudaMemcpy(grp.djobs, tab.data(), sizeof(GateJob) * tab.size(), cudaMemcpyHostToDevice);
+      if (cudaStreamCreateWithFlags(&grp.stream, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&grp.done, cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(ctx, HB_ERR_CUDA, "stream creation");
+    }
+    b->groups.push_back(grp);
+  }
+  if (!rc && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+    rc = fail(ctx, HB_ERR_CUDA, "event creation");
+  // capture: fork from the context stream, one persistent kernel per set on its own stream, join
+  if (!rc) {
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaEventRecord(b->fork, ctx->stream);
+    for (auto &grp : b->groups) {
+      if (e != cudaSuccess || rc) break;
+      e = cudaStreamWaitEvent(grp.stream, b->fork, 0);
+      if (e == cudaSuccess)
+        rc = launch_table_any(ctx, grp.keys, grp.keys->gates_per_cta, (const GateJob *)grp.djobs, grp.njobs,
+                              grp.batches, grp.grid, grp.stream);
+      if (e == cudaSuccess && !rc) e = cudaEventRecord(grp.done, grp.stream);
+      if (e == cudaSuccess && !rc) e = cudaStreamWaitEvent(ctx->stream, grp.done, 0);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
+    if (e == cudaSuccess) e = e2;
+    b->graph = g;
+    if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&b->exec, g, 0);
+    if (e != cudaSuccess && !rc) rc = cuda_fail(ctx, e, "batch graph capture");
+  }
+  if (rc) {
+    hb_batch_free(ctx, b);
+    return rc;
+  }
+  ctx->launches -= b->groups.size();  // capture is not execution: count launches when replayed
+  *out = b;
+  return HB_OK;
+}
+
+extern "C" int hb_batch_launch(hb_ctx *ctx, hb_batch *b) {
+  if (!ctx || !b || !b->exec) return HB_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaGraphLaunch(b->exec, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch graph launch");
+  ctx->launches += b->groups.size();
+  return HB_OK;
+}
+
+extern "C" int hb_batch_info(const hb_batch *b, uint64_t *gates, int *launches, int *grid_out, int grid_cap) {
+  if (!b) return HB_ERR_INVALID;
+  if (gates) *gates = b->gates;
+  if (launches) *launches = (int)b->groups.size();
+  for (int k = 0; grid_out && k < grid_cap && k < (int)b->groups.size(); ++k) grid_out[k] = (int)b->groups[k].grid;
+  return HB_OK;
+}
+

@@ -44,7 +44,8 @@ struct hb_keys {
   void *bsk = nullptr;
   void *ksk = nullptr;
   size_t bytes = 0;
-  int gates_per_cta = 4;  // persistent-kernel variant (autotuned)
+  int gates_per_cta = 4;    // persistent-kernel variant (autotuned)
+  double gates_per_s = 0;   // measured by hb_autotune (0: not calibrated)
 };
 
 namespace hbrt {

@@ -274,3 +274,92 @@ class Evaluator:
         check(lib().hb_bootstrap_lut(self.ctx.handle, self.keys.handle, _ptr(c), _ptr(lut),
                                      _ptr(out), len(c)), "bootstrap", self.ctx.handle)
         return out
+
+
+# ------------------------------------------------------------------------------------------------
+# Autotuning and mixed-set batches
+# ------------------------------------------------------------------------------------------------
+
+AUTOTUNE_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_autotune_cache.json")
+
+
+def _device_name(device):
+    try:
+        import torch
+        return torch.cuda.get_device_name(device)
+    except Exception:
+        return "cuda:%d" % device
+
+
+def _tune_key(ev):
+    r = ev.params.raw
+    return "|".join(str(x) for x in (_device_name(ev.ctx.device), r.field_id, r.ring_dim, r.lwe_dim,
+                                     r.br_bits, r.br_len, r.ks_bits, r.ks_len))
+
+
+def autotune(ev, sample_gates=0, use_cache=True):
+    """Pick the fastest compiled gates-per-CTA variant for this evaluator's key set (hb_autotune),
+    remembering the choice per device and parameter set in AUTOTUNE_CACHE."""
+    import json
+    key = _tune_key(ev)
+    cache = {}
+    if use_cache and os.path.exists(AUTOTUNE_CACHE):
+        try:
+            cache = json.load(open(AUTOTUNE_CACHE))
+        except ValueError:
+            cache = {}
+    if use_cache and key in cache:
+        if lib().hb_keys_set_gates_per_cta(ev.keys.handle, cache[key]["gates_per_cta"]) == 0:
+            return cache[key]["gates_per_cta"], cache[key]["gates_per_s"], True
+    g = ctypes.c_int()
+    rate = ctypes.c_double()
+    check(lib().hb_autotune(ev.ctx.handle, ev.keys.handle, sample_gates, ctypes.byref(g),
+                            ctypes.byref(rate)), "hb_autotune", ev.ctx.handle)
+    if use_cache:
+        cache[key] = {"gates_per_cta": g.value, "gates_per_s": rate.value}
+        tmp = AUTOTUNE_CACHE + ".tmp"
+        json.dump(cache, open(tmp, "w"), indent=1)
+        os.replace(tmp, AUTOTUNE_CACHE)
+    return g.value, rate.value, False
+
+
+class Batch:
+    """A planned batch of gate jobs that may mix parameter sets (hb_batch): one CUDA graph holding
+    one persistent launch per key set. jobs: iterable of (evaluator, gate_name, c0, c1, c2, out)
+    with torch CUDA tensors (c2 may be None)."""
+
+    def __init__(self, ctx: Context, jobs):
+        from ._lib import HbJob
+        jobs = list(jobs)
+        arr = (HbJob * max(1, len(jobs)))()
+        self._keep = jobs
+        for i, (ev, gate, c0, c1, c2, out) in enumerate(jobs):
+            arr[i].keys = ev.keys.handle
+            arr[i].gate = GATE_IDS[gate]
+            arr[i].count = c0.shape[0]
+            arr[i].c0 = c0.data_ptr()
+            arr[i].c1 = c1.data_ptr() if c1 is not None else None
+            arr[i].c2 = c2.data_ptr() if c2 is not None else None
+            arr[i].out = out.data_ptr()
+        h = ctypes.c_void_p()
+        check(lib().hb_batch_create(ctx.handle, arr, len(jobs), ctypes.byref(h)), "hb_batch_create",
+              ctx.handle)
+        self.ctx = ctx
+        self.handle = h
+
+    def info(self):
+        gates = ctypes.c_uint64()
+        launches = ctypes.c_int()
+        grid = (ctypes.c_int * 8)()
+        check(lib().hb_batch_info(self.handle, ctypes.byref(gates), ctypes.byref(launches), grid, 8),
+              "hb_batch_info")
+        return {"gates": gates.value, "launches": launches.value,
+                "sm_split": list(grid)[:launches.value]}
+
+    def launch(self):
+        check(lib().hb_batch_launch(self.ctx.handle, self.handle), "hb_batch_launch", self.ctx.handle)
+
+    def free(self):
+        if self.handle:
+            lib().hb_batch_free(self.ctx.handle, self.handle)
+            self.handle = None

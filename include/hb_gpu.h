@@ -165,6 +165,37 @@ int hb_external_product_device(hb_ctx *ctx, int field_id, uint32_t log_n, uint32
                                uint32_t len, const void *d_rgsw, const void *rlwe_in,
                                void *rlwe_out, size_t count);
 
+/* ---- autotuning and mixed-set batches ----------------------------------------------------- */
+
+/* Times every compiled gates-per-CTA variant of the persistent kernel for this key set on
+ * sample_gates NAND gates (0: 24 per SM) and keeps the fastest for later launches; reports the
+ * choice and its throughput. No counterpart in the reference (its path is single-threaded CPU). */
+int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, int *gates_per_cta,
+                double *gates_per_s);
+/* Restores a cached autotuner choice; HB_ERR_UNSUPPORTED if that variant is not compiled. */
+int hb_keys_set_gates_per_cta(hb_keys *keys, int gates_per_cta);
+int hb_keys_gates_per_cta(const hb_keys *keys);
+
+/* One bootstrapped-gate job of a batch: `count` gates (NAND..MAJORITY) of one key set on device
+ * buffers. Batching across gates of the reference's Evaluator (tfhe/src/bfhe/evaluate.rs:113-237). */
+typedef struct hb_job {
+  hb_keys *keys;
+  int32_t gate;
+  uint32_t count;
+  const void *c0, *c1, *c2;
+  void *out;
+} hb_job;
+typedef struct hb_batch hb_batch;
+
+/* Plans a batch of jobs that may mix parameter sets and gate kinds: one persistent launch per key
+ * set, SMs split across sets by estimated work, all captured into one CUDA graph. */
+int hb_batch_create(hb_ctx *ctx, const hb_job *jobs, size_t njobs, hb_batch **out);
+/* Enqueues the whole batch as one graph launch on the context stream. */
+int hb_batch_launch(hb_ctx *ctx, hb_batch *batch);
+void hb_batch_free(hb_ctx *ctx, hb_batch *batch);
+/* Gates in the batch, kernels per launch, and the SM share of each (up to grid_cap entries). */
+int hb_batch_info(const hb_batch *batch, uint64_t *gates, int *launches, int *grid, int grid_cap);
+
 /* Evaluator::mux for callers that cannot allocate device memory during a call: a serving process
  * that reserves its whole HBM budget at start-up and may not take a cudaMalloc on its request path
  * (cudaMalloc can synchronise the device and fragments the heap), or a host that hands out all

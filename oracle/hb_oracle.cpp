@@ -37,33 +37,29 @@ struct Gold {
 
   static T canon(T x) { return x >= P ? x - P : x; }
 
-  // 128-bit -> 64-bit folding using 2^64 = 2^32 - 1 and 2^96 = -1 (mod P).
-  // Result in [0, 2^64), not necessarily canonical.
+  // 128-bit -> 64-bit folding using 2^64 = 2^32 - 1 and 2^96 = -1 (mod P), written with 128-bit
+  // sums so the compiler emits no data-dependent branches. Result in [0, 2^64), not canonical.
   static T fold128(u128 x) {
-    T lo = (T)x;
-    T hi = (T)(x >> 64);
-    T hh = hi >> 32;
-    T hl = hi & EPS;
-    T t0 = lo - hh;
-    if (lo < hh) t0 -= EPS;  // wrapped by 2^64 (= EPS mod P): remove the EPS it added
-    T t1 = hl * EPS;
-    T r = t0 + t1;
-    if (r < t1) r += EPS;  // carry out of 2^64 is worth EPS; cannot carry twice
-    return r;
+    const T lo = (T)x;
+    const T hi = (T)(x >> 64);
+    const T hh = hi >> 32;
+    const T hl = hi & EPS;
+    u128 t = (u128)lo + (u128)hl * EPS + P - hh;  // x mod P plus P, below 2^66
+    const T tl = (T)t, th = (T)(t >> 64);          // th < 4
+    const u128 r = (u128)tl + (u128)th * EPS;      // below 2^64 + 2^34
+    return (T)r + (T)(r >> 64) * EPS;              // a carry leaves (T)r below 2^34: no overflow
   }
 
   // Canonical arithmetic.
   static T add(T a, T b) {
-    a = canon(a);
-    b = canon(b);
-    T s = a + b;
-    if (s < a || s >= P) s -= P;
-    return s;
+    const u128 s = (u128)canon(a) + canon(b);
+    return (T)(s >= P ? s - P : s);
   }
   static T sub(T a, T b) {
     a = canon(a);
     b = canon(b);
-    return a >= b ? a - b : a - b + P;
+    const T d = a - b;
+    return a >= b ? d : d + P;
   }
   static T mul(T a, T b) { return canon(fold128((u128)a * b)); }
   static T neg(T a) {
@@ -588,7 +584,11 @@ void external_product(const Ntt<F> &ntt, uint32_t bits, uint32_t L, const typena
                       typename F::T *ea, typename F::T *eb) {
   using T = typename F::T;
   const uint32_t N = ntt.n;
-  std::vector<T> ma(N, 0), mb(N, 0), poly(N), digit(N);
+  thread_local std::vector<T> ma, mb, poly, digit;
+  ma.assign(N, 0);
+  mb.assign(N, 0);
+  poly.resize(N);
+  digit.resize(N);
   for (uint32_t part = 0; part < 2; ++part) {
     const T *src = part == 0 ? ea : eb;
     std::copy(src, src + N, poly.begin());

@@ -1,0 +1,75 @@
+"""Autotuner and mixed-parameter-set batches (one graph launch) against single-set launches."""
+
+import numpy as np
+import pytest
+
+from gpu_util import empty_dev, from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(hb):
+    c = hb.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def evaluators(hb, ctx):
+    evs = {}
+    for pid in (0, 1, 2):
+        sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(pid), 0)
+        evs[pid] = (sk, hb.Evaluator(sk, ctx))
+    yield evs
+    for sk, ev in evs.values():
+        ev.keys.free()
+
+
+def test_autotune_picks_a_compiled_variant(hb, evaluators):
+    from hasteboots_b200._lib import lib
+    sk, ev = evaluators[0]
+    g, rate, cached = hb.autotune(ev, sample_gates=148 * 24, use_cache=False)
+    assert g in (4, 6, 8) and rate > 0
+    assert lib().hb_keys_gates_per_cta(ev.keys.handle) == g
+    assert lib().hb_keys_set_gates_per_cta(ev.keys.handle, 5) != 0  # not compiled
+
+
+def test_mixed_batch_equals_alone(hb, evaluators, ctx):
+    """Every job's outputs are identical alone (single-set launch) and inside the mixed graph."""
+    rng = np.random.default_rng(4)
+    gates = ["nand", "and", "or", "xor", "xnor", "nor", "majority"]
+    plan = []
+    for i in range(9):
+        pid = int(rng.integers(0, 3))
+        count = int(np.exp(rng.uniform(0, np.log(300))))
+        gate = gates[i % len(gates)]
+        plan.append((pid, gate, max(1, count)))
+    jobs, alone, expect = [], [], []
+    for i, (pid, gate, count) in enumerate(plan):
+        sk, ev = evaluators[pid]
+        bits = rng.integers(0, 2, (3, count)).astype(np.uint8)
+        cs = [sk.encrypt(bits[k], 100000 * (i + 1) + 1000 * k) for k in range(3)]
+        ds = [to_dev(c) for c in cs]
+        out = empty_dev(cs[0].shape, cs[0].dtype)
+        jobs.append((ev, gate, ds[0], ds[1], ds[2] if gate == "majority" else None, out))
+        fn = {"and": ev.and_, "or": ev.or_}.get(gate, getattr(ev, gate, None))
+        args = (cs[0], cs[1], cs[2]) if gate == "majority" else (cs[0], cs[1])
+        alone.append(fn(*args))
+        a, b, c = bits
+        expect.append({"nand": 1 - (a & b), "and": a & b, "or": a | b, "xor": a ^ b,
+                       "xnor": 1 - (a ^ b), "nor": 1 - (a | b),
+                       "majority": (a & b) | (b & c) | (a & c)}[gate])
+    batch = hb.Batch(ctx, jobs)
+    info = batch.info()
+    assert info["launches"] == len({p for p, _, _ in plan})
+    assert sum(info["sm_split"]) <= 148
+    for rep in range(2):
+        batch.launch()
+        ctx.synchronize()
+        for (pid, gate, count), job, ref, exp in zip(plan, jobs, alone, expect):
+            sk = evaluators[pid][0]
+            got = from_dev(job[5], ref.dtype)
+            assert (got == ref).all(), (pid, gate, count)
+            assert (sk.decrypt(got) == exp).all()
+    batch.free()
