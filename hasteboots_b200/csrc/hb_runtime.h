@@ -3,11 +3,16 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 #include <utility>
 #include <vector>
 
 #include "../../include/hb_gpu.h"
+
+namespace hb {
+struct GateJob;
+}
 
 namespace hbrt {
 
@@ -36,7 +41,7 @@ struct hb_ctx {
   std::string err;
   hbrt::DevTables tables[2][13];
   hbrt::Scratch jobs, io, mux_tmp, acc;
-  unsigned long long launches = 0;  // bootstrap kernel launches issued by this context
+  std::atomic<unsigned long long> launches{0};  // bootstrap kernel launches issued by this context
 };
 
 struct hb_keys {
@@ -57,4 +62,10 @@ int scratch(hb_ctx *ctx, Scratch &s, size_t bytes);
 int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out);
 int check_status(hb_ctx *ctx);
 long long wait_budget();
+// One persistent bootstrapping launch over a device job table (full grid, the keys' variant).
+int launch_set(hb_ctx *ctx, hb_keys *keys, const hb::GateJob *djobs, int njobs, uint32_t batches,
+               cudaStream_t stream);
+// The job record of `count` single-bootstrap gates (NAND..MAJORITY) of parameter set p.
+int gate_job(const hb_params &p, int gate, const void *c0, const void *c1, const void *c2, void *out,
+             uint32_t count, hb::GateJob *job);
 }  // namespace hbrt

@@ -363,3 +363,57 @@ class Batch:
         if self.handle:
             lib().hb_batch_free(self.ctx.handle, self.handle)
             self.handle = None
+
+
+class Server:
+    """Request loop with continuous batching (hb_serve_*). Submissions take host ciphertext arrays
+    (pinned memory recommended), which this wrapper keeps alive until fetched."""
+
+    def __init__(self, ctx: Context, hbm_budget=0, max_wave_gates=0, max_inflight_waves=0):
+        from ._lib import HbServeConfig
+        cfg = HbServeConfig(hbm_budget, max_wave_gates, max_inflight_waves)
+        h = ctypes.c_void_p()
+        check(lib().hb_serve_start(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)), "hb_serve_start",
+              ctx.handle)
+        self.ctx = ctx
+        self.handle = h
+        self._live = {}
+
+    def submit(self, ev: "Evaluator", gate, c0, c1, c2=None):
+        rid = ctypes.c_uint64()
+        arrays = [a for a in (c0, c1, c2) if a is not None]
+        check(lib().hb_serve_submit(self.handle, ev.keys.handle, GATE_IDS[gate], _ptr(c0), _ptr(c1),
+                                    _ptr(c2), len(c0), ctypes.byref(rid)), "hb_serve_submit")
+        self._live[rid.value] = (arrays, ev.params, len(c0))
+        return rid.value
+
+    def state(self, rid):
+        st = ctypes.c_int()
+        check(lib().hb_serve_poll(self.handle, rid, ctypes.byref(st)), "hb_serve_poll")
+        return st.value
+
+    def next_done(self, timeout=10.0):
+        rid = ctypes.c_uint64()
+        rc = lib().hb_serve_next_done(self.handle, ctypes.byref(rid), timeout)
+        return rid.value if rc == 0 else None
+
+    def fetch(self, rid, out=None):
+        arrays, params, count = self._live.pop(rid)
+        if out is None:
+            out = np.zeros((count, params.lwe_dimension() + 1), params.dtype)
+        lat = ctypes.c_double()
+        check(lib().hb_serve_fetch(self.handle, rid, _ptr(out), ctypes.byref(lat)), "hb_serve_fetch")
+        return out, lat.value
+
+    def stats(self):
+        from ._lib import HbServeStats
+        st = HbServeStats()
+        lib().hb_serve_stats(self.handle, ctypes.byref(st))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def stop(self):
+        if self.handle:
+            rc = lib().hb_serve_stop(self.handle)
+            self.handle = None
+            return rc
+        return 0

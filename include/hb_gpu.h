@@ -196,6 +196,39 @@ void hb_batch_free(hb_ctx *ctx, hb_batch *batch);
 /* Gates in the batch, kernels per launch, and the SM share of each (up to grid_cap entries). */
 int hb_batch_info(const hb_batch *batch, uint64_t *gates, int *launches, int *grid, int grid_cap);
 
+/* ---- serving: request loop with continuous batching ----------------------------------------
+ * No counterpart in the reference (its Evaluator is a synchronous single-gate CPU call). */
+
+typedef struct hb_server hb_server;
+typedef struct hb_serve_config {
+  size_t hbm_budget;           /* bytes of request memory (inputs + output) on the device; 0 = 120 GiB */
+  uint32_t max_wave_gates;     /* gates packed into one wave at most; 0 = no limit */
+  uint32_t max_inflight_waves; /* waves on the GPU at once (1..4); 0 = 2 */
+} hb_serve_config;
+typedef struct hb_serve_stats {
+  uint64_t submitted, admitted, completed, failed, queued, waves, gates_completed;
+  double p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s;
+  double gates_per_s; /* completed gates / (last completion - first submission) */
+  size_t hbm_in_use, hbm_peak;
+} hb_serve_statistics;
+
+/* Starts the request loop of a context (one worker thread). Keys used by requests must outlive it. */
+int hb_serve_start(hb_ctx *ctx, const hb_serve_config *cfg, hb_server **out);
+/* Queues `count` single-bootstrap gates (NAND..MAJORITY) on host input buffers, which must stay
+ * valid until the request is admitted (its state leaves 0). Thread-safe. */
+int hb_serve_submit(hb_server *s, hb_keys *keys, int gate, const void *c0, const void *c1,
+                    const void *c2, uint32_t count, uint64_t *id);
+/* State of a request: 0 queued, 1 admitted, 2 running, 3 done, -1 failed. */
+int hb_serve_poll(hb_server *s, uint64_t id, int *state);
+/* Id of the next request to finish (done or failed), waiting up to timeout_s; HB_ERR_BUSY on timeout. */
+int hb_serve_next_done(hb_server *s, uint64_t *id, double timeout_s);
+/* Copies a finished request's output ciphertexts to `out` (host, may be NULL), reports its latency
+ * (submission to completion on the device) and returns its memory to the budget. */
+int hb_serve_fetch(hb_server *s, uint64_t id, void *out, double *latency_s);
+int hb_serve_stats(hb_server *s, hb_serve_statistics *out);
+/* Stops admitting, lets the waves on the GPU finish, cancels the rest and frees everything. */
+int hb_serve_stop(hb_server *s);
+
 /* Evaluator::mux for callers that cannot allocate device memory during a call: a serving process
  * that reserves its whole HBM budget at start-up and may not take a cudaMalloc on its request path
  * (cudaMalloc can synchronise the device and fragments the heap), or a host that hands out all
