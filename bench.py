@@ -41,6 +41,24 @@ def modmuls_per_gate(N, n, length, ks_len):
     return n * ((2 * length + 2) * ntt + 4 * length * N) + ((ks_len + 2) * ntt + 2 * ks_len * N)
 
 
+def reduce_max(x, world):
+    """Max of a per-rank float over all ranks (the step time every replica must wait for)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(ms_per_step_local, gates_per_rank, world):
+    """Whole-job throughput of `world` replicas: all ranks' gates over the slowest rank's step."""
+    ms = reduce_max(ms_per_step_local, world)
+    return ms, gates_per_rank * world / (ms / 1e3)
+
+
 def dist_env():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
             int(os.environ.get("LOCAL_RANK", 0)))
@@ -229,7 +247,8 @@ def workload_mixed(args):
             "config": {"workload": "64 jobs, log-uniform 1-4096 gates, sets uniform over ZAMA/GOLDILOCKS/BABYBEAR",
                        "gates": info["gates"], "kernels_per_graph": info["launches"],
                        "sm_split": info["sm_split"],
-                       "autotuned_gates_per_cta": {str(k): v[0] for k, v in tuned.items()},
+                       "autotuned_variant": {str(k): {"threads_per_gate": v[0][0], "gates_per_cta": v[0][1]}
+                                             for k, v in tuned.items()},
                        "autotuned_gates_per_s": {str(k): v[1] for k, v in tuned.items()}},
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "checks": {"truth_tables": bool(ok)}}
@@ -492,7 +511,7 @@ def main():
         check(L.hb_gate_device(ctx.handle, ev.keys.handle, GATE_NAND, d0.data_ptr(), d1.data_ptr(),
                                None, dout.data_ptr(), G), "hb_gate_device", ctx.handle)
 
-    tuned_g, tuned_rate, tuned_cached = tfhe.autotune(ev)  # setup, outside the timed region
+    (tuned_t, tuned_g), tuned_rate, tuned_cached = tfhe.autotune(ev)  # setup, outside the timed region
     # roofline denominator: measured field-multiplication throughput of this GPU
     probe = ctypes.c_double()
     check(L.hb_probe_modmul(ctx.handle, raw.field_id, ctypes.byref(probe)), "probe", ctx.handle)
@@ -513,13 +532,7 @@ def main():
         ev1.synchronize()
         ctx.synchronize()
     launches = L.hb_ctx_launches(ctx.handle) - launches0
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_per_step = ms / args.steps
-    value = G * world / (ms_per_step / 1e3)
+    ms_per_step, value = aggregate(ev0.elapsed_time(ev1) / args.steps, G, world)
 
     # correctness of the timed outputs: NAND truth table on every gate
     out = dout.cpu().numpy().view(params.dtype).reshape(G, width)
@@ -540,11 +553,7 @@ def main():
     if not e2e_times:  # e2e leg disabled (profiling runs): reuse the device outputs
         pout.copy_(torch.from_numpy(out.view(ivt)))
         e2e_times = [float("nan")]
-    e2e_s = max(e2e_times)
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = reduce_max(max(e2e_times), world)
     e2e_ok = bool((pout.numpy().view(params.dtype).reshape(G, width) == out).all())
 
     # plain one-gate-per-launch form on a sample of the same gates
@@ -598,7 +607,7 @@ def main():
             "gates_per_gpu": G,
             "parallelism": f"replicas x{world}",
             "l2": "inputs (191 MB) and BSK (191 MB) exceed L2; no flush",
-            "gates_per_cta": tuned_g,
+            "kernel_variant": {"threads_per_gate": tuned_t, "gates_per_cta": tuned_g},
             "autotune": {"gates_per_s_sample": tuned_rate, "from_cache": tuned_cached},
         },
         "latency_ms": {"p50": ms_per_step, "p99": ms_per_step,

@@ -23,8 +23,8 @@ EXPORTS = [
     "hb_ctx_synchronize", "hb_ctx_hbm_in_use", "hb_keys_upload", "hb_keys_free", "hb_keys_params",
     "hb_gate", "hb_gate_device", "hb_gate_device_plain", "hb_bootstrap_lut",
     "hb_ntt_forward_device", "hb_ntt_inverse_device", "hb_ntt_roundtrip_device", "hb_rgsw_upload",
-    "hb_rgsw_free", "hb_external_product_device", "hb_autotune", "hb_keys_set_gates_per_cta",
-    "hb_keys_gates_per_cta", "hb_batch_create", "hb_batch_launch", "hb_batch_free",
+    "hb_rgsw_free", "hb_external_product_device", "hb_autotune", "hb_keys_set_config",
+    "hb_keys_config", "hb_batch_create", "hb_batch_launch", "hb_batch_free",
     "hb_batch_info", "hb_serve_start", "hb_serve_submit", "hb_serve_poll", "hb_serve_next_done",
     "hb_serve_fetch", "hb_serve_stats", "hb_serve_stop", "hb_gate_mux_device_noalloc",
     "hb_probe_modmul", "hb_ctx_launches",
@@ -118,9 +118,10 @@ def lib():
         "hb_rgsw_upload": (i32, [vp, i32, u32, u32, u32, vp, pp]),
         "hb_rgsw_free": (None, [vp, vp]),
         "hb_external_product_device": (i32, [vp, i32, u32, u32, u32, vp, vp, vp, sz]),
-        "hb_autotune": (i32, [vp, vp, u32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]),
-        "hb_keys_set_gates_per_cta": (i32, [vp, i32]),
-        "hb_keys_gates_per_cta": (i32, [vp]),
+        "hb_autotune": (i32, [vp, vp, u32, ctypes.POINTER(i32), ctypes.POINTER(i32),
+                              ctypes.POINTER(ctypes.c_double)]),
+        "hb_keys_set_config": (i32, [vp, vp, i32, i32]),
+        "hb_keys_config": (i32, [vp, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "hb_batch_create": (i32, [vp, ctypes.POINTER(HbJob), sz, pp]),
         "hb_batch_launch": (i32, [vp, vp]),
         "hb_batch_free": (None, [vp, vp]),

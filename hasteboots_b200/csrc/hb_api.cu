@@ -89,10 +89,9 @@ uint32_t brv(uint32_t x, uint32_t bits) {
 // stage follows GroupNtt::fwd_stage / inv_stage (hb_ntt.cuh): the twiddle of block i = high*K + k
 // is stored at stage_base + k * (stage_size / K) + high.
 template <class F>
-int build_tables(hb_ctx *ctx, uint32_t logn, DevTables &t) {
+int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
   using W = typename F::W;
   const uint32_t N = 1u << logn;
-  const uint32_t logv = 4;  // every compiled group NTT holds 16 words per thread
   const uint32_t V = 1u << logv;
   const uint64_t order = (uint64_t)F::P - 1;
   if (order % (2ull * N)) return fail(ctx, HB_ERR_UNSUPPORTED, "2N does not divide Q-1");
@@ -164,13 +163,13 @@ int build_tables(hb_ctx *ctx, uint32_t logn, DevTables &t) {
   return HB_OK;
 }
 
-int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out) {
-  if (logn < 6 || logn > 12 || (field_id != 0 && field_id != 1))
+int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out, uint32_t logv) {
+  if (logn < 6 || logn > 12 || logv < 1 || logv > 5 || (field_id != 0 && field_id != 1))
     return fail(ctx, HB_ERR_UNSUPPORTED, "no NTT tables for field %d log_n %u", field_id, logn);
-  DevTables &t = ctx->tables[field_id][logn];
+  DevTables &t = ctx->tables[field_id][logn][logv];
   if (!t.tw) {
-    int rc = field_id == HB_FIELD_GOLDILOCKS ? build_tables<Goldilocks>(ctx, logn, t)
-                                             : build_tables<BabyBear>(ctx, logn, t);
+    int rc = field_id == HB_FIELD_GOLDILOCKS ? build_tables<Goldilocks>(ctx, logn, logv, t)
+                                             : build_tables<BabyBear>(ctx, logn, logv, t);
     if (rc) return rc;
   }
   *out = &t;
@@ -207,7 +206,7 @@ constexpr int kStages = 3;
 template <class F, int LOGN, int T>
 int launch_prepare(hb_ctx *ctx, const void *d_in, void *d_out, size_t npolys) {
   DevTables *tb;
-  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb);
+  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb, hb::GroupNtt<F, LOGN, T>::LOGV);
   if (rc) return rc;
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
@@ -221,17 +220,22 @@ int launch_prepare(hb_ctx *ctx, const void *d_in, void *d_out, size_t npolys) {
   return e == cudaSuccess ? HB_OK : cuda_fail(ctx, e, "prepare_polys launch");
 }
 
+// Key polynomials are laid out for a group of T threads (slot t*V + v stored at v*T + t).
 template <class F>
-int prepare_any(hb_ctx *ctx, uint32_t logn, const void *d_in, void *d_out, size_t npolys) {
-  if (logn == 10) return launch_prepare<F, 10, 64>(ctx, d_in, d_out, npolys);
-  if (logn == 11) return launch_prepare<F, 11, 128>(ctx, d_in, d_out, npolys);
-  return fail(ctx, HB_ERR_UNSUPPORTED, "ring dimension 2^%u has no compiled kernel", logn);
+int prepare_any(hb_ctx *ctx, uint32_t logn, int T, const void *d_in, void *d_out, size_t npolys) {
+  if (logn == 10 && T == 64) return launch_prepare<F, 10, 64>(ctx, d_in, d_out, npolys);
+  if (logn == 10 && T == 128) return launch_prepare<F, 10, 128>(ctx, d_in, d_out, npolys);
+  if (logn == 11 && T == 128) return launch_prepare<F, 11, 128>(ctx, d_in, d_out, npolys);
+  return fail(ctx, HB_ERR_UNSUPPORTED, "ring dimension 2^%u with %d threads has no compiled kernel", logn, T);
 }
 
-int prepare_field(hb_ctx *ctx, int field, uint32_t logn, const void *d_in, void *d_out, size_t npolys) {
-  return field == HB_FIELD_GOLDILOCKS ? prepare_any<Goldilocks>(ctx, logn, d_in, d_out, npolys)
-                                      : prepare_any<BabyBear>(ctx, logn, d_in, d_out, npolys);
+int prepare_field(hb_ctx *ctx, int field, uint32_t logn, int T, const void *d_in, void *d_out, size_t npolys) {
+  return field == HB_FIELD_GOLDILOCKS ? prepare_any<Goldilocks>(ctx, logn, T, d_in, d_out, npolys)
+                                      : prepare_any<BabyBear>(ctx, logn, T, d_in, d_out, npolys);
 }
+
+// The standard group size of the NTT and external-product kernels (16 words per thread).
+int std_threads(uint32_t logn) { return logn == 10 ? 64 : 128; }
 
 template <class F, int LOGN, int T, int GPB>
 int launch_ntt(hb_ctx *ctx, const void *in, void *out, size_t count, int mode) {
@@ -241,6 +245,7 @@ int launch_ntt(hb_ctx *ctx, const void *in, void *out, size_t count, int mode) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   auto kern = hb::ntt_batch_kernel<F, LOGN, T, GPB>;
+  static_assert(hb::GroupNtt<F, LOGN, T>::LOGV == 4, "NTT kernels use the 16-word tables");
   const size_t smem = sizeof(W) * (2 * N + GPB * 2 * N);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
@@ -273,6 +278,7 @@ int launch_ext(hb_ctx *ctx, const void *rgsw, uint32_t bits, uint32_t len, const
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   auto kern = hb::ext_product_kernel<F, LOGN, T, G, kStages>;
+  static_assert(hb::GroupNtt<F, LOGN, T>::LOGV == 4, "external-product kernels use the 16-word tables");
   const size_t smem = sizeof(W) * (2 * N + kStages * 2 * N + G * 2 * N) + sizeof(uint64_t) * kStages + 16;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const size_t batches = (count + G - 1) / G;
@@ -340,7 +346,7 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   DevTables *tb;
-  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb);
+  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb, hb::GroupNtt<F, LOGN, T>::LOGV);
   if (rc) return rc;
   // Batched: jobs are laid end to end in batch space. Plain: every launch holds one job whose
   // batches start at 0.
@@ -399,33 +405,36 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
   return HB_OK;
 }
 
-// Compiled gates-per-CTA variants of the persistent batched kernel (T = 64 threads per gate).
-// keys->gates_per_cta selects one (autotuned per parameter set, hb_autotune).
+// Compiled variants of the persistent bootstrapping kernel: (field, threads per gate T, gates per
+// CTA G). The key layout fixes T at upload; the autotuner picks G among the variants of that T.
+// G = 1 is the plain one-gate-per-launch form.
+#define HB_BOOT_VARIANTS(X)                                                                    \
+  X(Goldilocks, 64, 1) X(Goldilocks, 64, 3) X(Goldilocks, 64, 4) X(Goldilocks, 128, 1)        \
+  X(Goldilocks, 128, 3) X(Goldilocks, 128, 4) X(BabyBear, 64, 1) X(BabyBear, 64, 4)           \
+  X(BabyBear, 64, 6) X(BabyBear, 64, 8) X(BabyBear, 128, 1) X(BabyBear, 128, 4) X(BabyBear, 128, 6)
+
+template <class F>
+constexpr int field_of() { return F::FIELD_ID; }
+
 int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain) {
   if (keys->p.ring_dim != 1024)
     return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
-  const int G = keys->gates_per_cta;
-  if (keys->p.field_id == HB_FIELD_GOLDILOCKS) {
-    if (plain) return launch_boot<Goldilocks, 10, 64, 1>(ctx, keys, jobs, true);
-    switch (G) {
-      case 3: return launch_boot<Goldilocks, 10, 64, 3>(ctx, keys, jobs, false);
-      case 4: return launch_boot<Goldilocks, 10, 64, 4>(ctx, keys, jobs, false);
-    }
-  } else {
-    if (plain) return launch_boot<BabyBear, 10, 64, 1>(ctx, keys, jobs, true);
-    switch (G) {
-      case 4: return launch_boot<BabyBear, 10, 64, 4>(ctx, keys, jobs, false);
-      case 6: return launch_boot<BabyBear, 10, 64, 6>(ctx, keys, jobs, false);
-      case 8: return launch_boot<BabyBear, 10, 64, 8>(ctx, keys, jobs, false);
-    }
-  }
-  return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
+  const int G = plain ? 1 : keys->gates_per_cta, T = keys->threads_per_gate, fld = keys->p.field_id;
+#define HB_CASE(FLD, TT, GG) \
+  if (fld == field_of<FLD>() && T == TT && G == GG) return launch_boot<FLD, 10, TT, GG>(ctx, keys, jobs, plain);
+  HB_BOOT_VARIANTS(HB_CASE)
+#undef HB_CASE
+  return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d threads per gate and %d gates per CTA", T, G);
 }
 
-// Gates-per-CTA variants compiled for each field (the autotuner's candidates).
-const std::vector<int> &variants(int field_id) {
-  static const std::vector<int> gl = {3, 4}, bb = {4, 6, 8};
-  return field_id == HB_FIELD_GOLDILOCKS ? gl : bb;
+// Gates-per-CTA variants compiled for a field and group size (the autotuner's candidates).
+std::vector<int> variants(int field_id, int T) {
+  std::vector<int> v;
+#define HB_CASE(FLD, TT, GG) \
+  if (field_id == field_of<FLD>() && T == TT && GG > 1) v.push_back(GG);
+  HB_BOOT_VARIANTS(HB_CASE)
+#undef HB_CASE
+  return v;
 }
 
 uint32_t batches_of(const std::vector<GateJob> &jobs, int G) {
@@ -441,7 +450,7 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   DevTables *tb;
-  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb);
+  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb, hb::GroupNtt<F, LOGN, T>::LOGV);
   if (rc) return rc;
   hb::BootParams<W> prm{};
   prm.bsk = (const W *)keys->bsk;
@@ -473,15 +482,13 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
 
 int launch_table_any(hb_ctx *ctx, hb_keys *keys, int G, const GateJob *djobs, int njobs,
                      uint32_t batches, unsigned grid, cudaStream_t stream) {
-  if (keys->p.field_id == HB_FIELD_GOLDILOCKS) {
-    if (G == 3) return launch_table<Goldilocks, 10, 64, 3>(ctx, keys, djobs, njobs, batches, grid, stream);
-    if (G == 4) return launch_table<Goldilocks, 10, 64, 4>(ctx, keys, djobs, njobs, batches, grid, stream);
-  } else {
-    if (G == 4) return launch_table<BabyBear, 10, 64, 4>(ctx, keys, djobs, njobs, batches, grid, stream);
-    if (G == 6) return launch_table<BabyBear, 10, 64, 6>(ctx, keys, djobs, njobs, batches, grid, stream);
-    if (G == 8) return launch_table<BabyBear, 10, 64, 8>(ctx, keys, djobs, njobs, batches, grid, stream);
-  }
-  return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
+  const int T = keys->threads_per_gate, fld = keys->p.field_id;
+#define HB_CASE(FLD, TT, GG)                                   \
+  if (fld == field_of<FLD>() && T == TT && G == GG && GG > 1) \
+    return launch_table<FLD, 10, TT, GG>(ctx, keys, djobs, njobs, batches, grid, stream);
+  HB_BOOT_VARIANTS(HB_CASE)
+#undef HB_CASE
+  return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d threads per gate and %d gates per CTA", T, G);
 }
 
 bool single_bootstrap_gate(int gate) { return gate >= HB_GATE_NAND && gate <= HB_GATE_MAJORITY; }
@@ -498,6 +505,12 @@ __global__ void lwe_not_kernel(const typename F::W *in, typename F::W *out, size
 }
 
 size_t word_size(const hb_params &p) { return p.field_id == HB_FIELD_GOLDILOCKS ? 8 : 4; }
+
+int default_threads_per_gate(int field_id) {
+  const char *env = getenv("HB_THREADS_PER_GATE");
+  if (env && (atoi(env) == 64 || atoi(env) == 128)) return atoi(env);
+  return field_id == HB_FIELD_GOLDILOCKS ? 64 : 64;
+}
 
 int default_gates_per_cta(int field_id) {
   const char *env = getenv("HB_GATES_PER_CTA");
@@ -591,11 +604,14 @@ int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void 
     delete k;
     return rc;
   }
+  k->threads_per_gate = default_threads_per_gate(p->field_id);
   cudaError_t e = cudaMemcpyAsync(staging, bsk, nb * ws, cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess) rc = prepare_field(ctx, p->field_id, logn, staging, k->bsk, nb / p->ring_dim);
+  if (e == cudaSuccess)
+    rc = prepare_field(ctx, p->field_id, logn, k->threads_per_gate, staging, k->bsk, nb / p->ring_dim);
   if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess && !rc) e = cudaMemcpyAsync(staging, ksk, nk * ws, cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess && !rc) rc = prepare_field(ctx, p->field_id, logn, staging, k->ksk, nk / p->ring_dim);
+  if (e == cudaSuccess && !rc)
+    rc = prepare_field(ctx, p->field_id, logn, k->threads_per_gate, staging, k->ksk, nk / p->ring_dim);
   if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(ctx->stream);
   dev_free(ctx, staging);
   if (e != cudaSuccess || rc) {
@@ -606,6 +622,10 @@ int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void 
   }
   k->bytes = (nb + nk) * ws;
   k->gates_per_cta = default_gates_per_cta(p->field_id);
+  if (variants(p->field_id, k->threads_per_gate).size() &&
+      std::find(variants(p->field_id, k->threads_per_gate).begin(), variants(p->field_id, k->threads_per_gate).end(),
+                k->gates_per_cta) == variants(p->field_id, k->threads_per_gate).end())
+    k->gates_per_cta = variants(p->field_id, k->threads_per_gate).back();
   *out = k;
   return HB_OK;
 }
@@ -778,7 +798,7 @@ int hb_rgsw_upload(hb_ctx *ctx, int field_id, uint32_t log_n, uint32_t bits, uin
     return rc;
   }
   cudaMemcpyAsync(staging, rgsw, words * ws, cudaMemcpyHostToDevice, ctx->stream);
-  rc = prepare_field(ctx, field_id, log_n, staging, dst, words / N);
+  rc = prepare_field(ctx, field_id, log_n, std_threads(log_n), staging, dst, words / N);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   dev_free(ctx, staging);
   if (rc || e != cudaSuccess) {
@@ -918,15 +938,12 @@ int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJo
 
 int noalloc_layer(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJob *djobs, int njobs,
                   uint32_t batches, int *dstatus) {
-  const int G = keys->gates_per_cta;
-  if (keys->p.field_id == HB_FIELD_GOLDILOCKS) {
-    if (G == 3) return launch_noalloc<Goldilocks, 10, 64, 3>(ctx, keys, tb, djobs, njobs, batches, dstatus);
-    if (G == 4) return launch_noalloc<Goldilocks, 10, 64, 4>(ctx, keys, tb, djobs, njobs, batches, dstatus);
-  } else {
-    if (G == 4) return launch_noalloc<BabyBear, 10, 64, 4>(ctx, keys, tb, djobs, njobs, batches, dstatus);
-    if (G == 6) return launch_noalloc<BabyBear, 10, 64, 6>(ctx, keys, tb, djobs, njobs, batches, dstatus);
-    if (G == 8) return launch_noalloc<BabyBear, 10, 64, 8>(ctx, keys, tb, djobs, njobs, batches, dstatus);
-  }
+  const int G = keys->gates_per_cta, T = keys->threads_per_gate, fld = keys->p.field_id;
+#define HB_CASE(FLD, TT, GG)                                   \
+  if (fld == field_of<FLD>() && T == TT && G == GG && GG > 1) \
+    return launch_noalloc<FLD, 10, TT, GG>(ctx, keys, tb, djobs, njobs, batches, dstatus);
+  HB_BOOT_VARIANTS(HB_CASE)
+#undef HB_CASE
   return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
 }
 
@@ -949,7 +966,8 @@ extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
   // The NTT tables were built when the keys were uploaded; this path must not build (allocate) them.
-  const DevTables *tb = &ctx->tables[p.field_id][10];
+  const int lv = keys->threads_per_gate == 128 ? 3 : 4;
+  const DevTables *tb = &ctx->tables[p.field_id][10][lv];
   if (!tb->tw) return fail(ctx, HB_ERR_INVALID, "keys were not uploaded on this context");
   unsigned char *base = nullptr;
   int rc = noalloc_address(ctx, &base);
@@ -996,20 +1014,78 @@ extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void
 // Autotuner and mixed-set batches
 // ------------------------------------------------------------------------------------------
 
-extern "C" int hb_keys_set_gates_per_cta(hb_keys *keys, int gates_per_cta) {
-  if (!keys) return HB_ERR_INVALID;
-  for (int g : variants(keys->p.field_id))
-    if (g == gates_per_cta) {
-      keys->gates_per_cta = g;
-      return HB_OK;
-    }
-  return HB_ERR_UNSUPPORTED;
+namespace {
+
+// Re-lays the device keys out for groups of T threads (stream-ordered on the context stream).
+int relayout_keys(hb_ctx *ctx, hb_keys *keys, int T) {
+  if (keys->threads_per_gate == T) return HB_OK;
+  const size_t ws = word_size(keys->p);
+  size_t nb = 0, nk = 0;
+  hb_params_sizes(&keys->p, nullptr, nullptr, &nb, &nk, nullptr);
+  uint32_t logn = 0;
+  while ((1u << logn) < keys->p.ring_dim) ++logn;
+  DevTables *tb;
+  const uint32_t logv = logn - (T == 128 ? 7 : 6);
+  int rc = tables(ctx, keys->p.field_id, logn, &tb, logv);  // the new group size's twiddles
+  void *nbsk = nullptr, *nksk = nullptr;
+  if (!rc) rc = dev_alloc(ctx, nb * ws, &nbsk);
+  if (!rc) rc = dev_alloc(ctx, nk * ws, &nksk);
+  if (rc) {
+    dev_free(ctx, nbsk);
+    return rc;
+  }
+  const unsigned grid = (unsigned)ctx->sms * 8;
+  const int N = (int)keys->p.ring_dim, Tf = keys->threads_per_gate;
+  if (ws == 8) {
+    hb::relayout_kernel<uint64_t><<<grid, 256, 0, ctx->stream>>>((const uint64_t *)keys->bsk, (uint64_t *)nbsk, nb, N, Tf, T);
+    hb::relayout_kernel<uint64_t><<<grid, 256, 0, ctx->stream>>>((const uint64_t *)keys->ksk, (uint64_t *)nksk, nk, N, Tf, T);
+  } else {
+    hb::relayout_kernel<uint32_t><<<grid, 256, 0, ctx->stream>>>((const uint32_t *)keys->bsk, (uint32_t *)nbsk, nb, N, Tf, T);
+    hb::relayout_kernel<uint32_t><<<grid, 256, 0, ctx->stream>>>((const uint32_t *)keys->ksk, (uint32_t *)nksk, nk, N, Tf, T);
+  }
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    dev_free(ctx, nbsk);
+    dev_free(ctx, nksk);
+    return cuda_fail(ctx, e, "key relayout");
+  }
+  dev_free(ctx, keys->bsk);
+  dev_free(ctx, keys->ksk);
+  keys->bsk = nbsk;
+  keys->ksk = nksk;
+  keys->threads_per_gate = T;
+  return HB_OK;
 }
 
-extern "C" int hb_keys_gates_per_cta(const hb_keys *keys) { return keys ? keys->gates_per_cta : 0; }
+bool compiled(int field_id, int T, int G) {
+  for (int g : variants(field_id, T))
+    if (g == G) return true;
+  return false;
+}
 
-extern "C" int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, int *chosen,
-                           double *gates_per_s) {
+}  // namespace
+
+extern "C" int hb_keys_set_config(hb_ctx *ctx, hb_keys *keys, int threads_per_gate, int gates_per_cta) {
+  if (!ctx || !keys) return HB_ERR_INVALID;
+  if (!compiled(keys->p.field_id, threads_per_gate, gates_per_cta))
+    return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d threads per gate and %d gates per CTA",
+                threads_per_gate, gates_per_cta);
+  cudaSetDevice(ctx->device);
+  int rc = relayout_keys(ctx, keys, threads_per_gate);
+  if (rc) return rc;
+  keys->gates_per_cta = gates_per_cta;
+  return HB_OK;
+}
+
+extern "C" int hb_keys_config(const hb_keys *keys, int *threads_per_gate, int *gates_per_cta) {
+  if (!keys) return HB_ERR_INVALID;
+  if (threads_per_gate) *threads_per_gate = keys->threads_per_gate;
+  if (gates_per_cta) *gates_per_cta = keys->gates_per_cta;
+  return HB_OK;
+}
+
+extern "C" int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, int *chosen_threads,
+                           int *chosen, double *gates_per_s) {
   if (!ctx || !keys) return HB_ERR_INVALID;
   if (keys->p.ring_dim != 1024) return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
   cudaSetDevice(ctx->device);
@@ -1027,9 +1103,12 @@ extern "C" int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, in
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  int best_g = keys->gates_per_cta;
+  int best_g = keys->gates_per_cta, best_t = keys->threads_per_gate;
   double best_rate = 0;
-  for (int G : variants(keys->p.field_id)) {
+  for (int T : {64, 128})
+  for (int G : variants(keys->p.field_id, T)) {
+    if (!rc) rc = relayout_keys(ctx, keys, T);
+    if (rc) break;
     std::vector<GateJob> jobs{keys->p.field_id == HB_FIELD_GOLDILOCKS
                                   ? make_job<Goldilocks>(HB_GATE_NAND, 1024, buf, buf, nullptr,
                                                          (char *)buf + bytes, sample_gates)
@@ -1053,6 +1132,7 @@ extern "C" int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, in
     if (rate > best_rate) {
       best_rate = rate;
       best_g = G;
+      best_t = T;
     }
   }
   cudaEventDestroy(e0);
@@ -1060,9 +1140,11 @@ extern "C" int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, in
   dev_free(ctx, buf);
   dev_free(ctx, tab);
   if (!rc) rc = check_status(ctx);
+  if (!rc) rc = relayout_keys(ctx, keys, best_t);
   if (rc) return rc;
   keys->gates_per_cta = best_g;
   keys->gates_per_s = best_rate;
+  if (chosen_threads) *chosen_threads = best_t;
   if (chosen) *chosen = best_g;
   if (gates_per_s) *gates_per_s = best_rate;
   return HB_OK;

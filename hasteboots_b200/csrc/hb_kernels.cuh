@@ -158,6 +158,22 @@ __global__ void __launch_bounds__(2 * T) prepare_polys_kernel(const typename F::
   }
 }
 
+// Moves key polynomials from the slot layout of a T_from-thread group to that of a T_to-thread
+// group: slot s = t*V + v is stored at v*T + t (V = N/T).
+template <class W>
+__global__ void __launch_bounds__(256) relayout_kernel(const W *__restrict__ in, W *__restrict__ out,
+                                                       unsigned long long words, int N, int t_from,
+                                                       int t_to) {
+  const int v_from = N / t_from, v_to = N / t_to;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < words;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long base = i - i % N;
+    const int p = (int)(i % N);
+    const int slot = (p % t_from) * v_from + p / t_from;
+    out[base + (slot % v_to) * t_to + slot / v_to] = in[i];
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Batched NTT kernels (one polynomial per thread group)
 // ------------------------------------------------------------------------------------------

@@ -39,7 +39,7 @@ struct hb_ctx {
   size_t in_use = 0;
   std::vector<std::pair<void *, size_t>> sizes;
   std::string err;
-  hbrt::DevTables tables[2][13];
+  hbrt::DevTables tables[2][13][6];  // [field][log2 N][log2 words per thread]
   hbrt::Scratch jobs, io, mux_tmp, acc;
   std::atomic<unsigned long long> launches{0};  // bootstrap kernel launches issued by this context
 };
@@ -49,7 +49,8 @@ struct hb_keys {
   void *bsk = nullptr;
   void *ksk = nullptr;
   size_t bytes = 0;
-  int gates_per_cta = 4;    // persistent-kernel variant (autotuned)
+  int threads_per_gate = 64;  // T: key slot layout and kernel group size
+  int gates_per_cta = 4;      // persistent-kernel variant (autotuned)
   double gates_per_s = 0;   // measured by hb_autotune (0: not calibrated)
 };
 
@@ -59,7 +60,7 @@ int cuda_fail(hb_ctx *ctx, cudaError_t e, const char *what);
 int dev_alloc(hb_ctx *ctx, size_t bytes, void **out);
 void dev_free(hb_ctx *ctx, void *p);
 int scratch(hb_ctx *ctx, Scratch &s, size_t bytes);
-int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out);
+int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out, uint32_t logv = 4);
 int check_status(hb_ctx *ctx);
 long long wait_budget();
 // One persistent bootstrapping launch over a device job table (full grid, the keys' variant).

@@ -298,8 +298,9 @@ def _tune_key(ev):
 
 
 def autotune(ev, sample_gates=0, use_cache=True):
-    """Pick the fastest compiled gates-per-CTA variant for this evaluator's key set (hb_autotune),
-    remembering the choice per device and parameter set in AUTOTUNE_CACHE."""
+    """Pick the fastest compiled kernel variant -- threads per gate (NTT tile) and gates per CTA --
+    for this evaluator's key set (hb_autotune), remembering the choice per device and parameter set
+    in AUTOTUNE_CACHE. Returns ((threads_per_gate, gates_per_cta), gates_per_s, from_cache)."""
     import json
     key = _tune_key(ev)
     cache = {}
@@ -308,19 +309,22 @@ def autotune(ev, sample_gates=0, use_cache=True):
             cache = json.load(open(AUTOTUNE_CACHE))
         except ValueError:
             cache = {}
-    if use_cache and key in cache:
-        if lib().hb_keys_set_gates_per_cta(ev.keys.handle, cache[key]["gates_per_cta"]) == 0:
-            return cache[key]["gates_per_cta"], cache[key]["gates_per_s"], True
+    if use_cache and key in cache and "threads_per_gate" in cache[key]:
+        c = cache[key]
+        if lib().hb_keys_set_config(ev.ctx.handle, ev.keys.handle, c["threads_per_gate"],
+                                    c["gates_per_cta"]) == 0:
+            return (c["threads_per_gate"], c["gates_per_cta"]), c["gates_per_s"], True
+    t = ctypes.c_int()
     g = ctypes.c_int()
     rate = ctypes.c_double()
-    check(lib().hb_autotune(ev.ctx.handle, ev.keys.handle, sample_gates, ctypes.byref(g),
-                            ctypes.byref(rate)), "hb_autotune", ev.ctx.handle)
+    check(lib().hb_autotune(ev.ctx.handle, ev.keys.handle, sample_gates, ctypes.byref(t),
+                            ctypes.byref(g), ctypes.byref(rate)), "hb_autotune", ev.ctx.handle)
     if use_cache:
-        cache[key] = {"gates_per_cta": g.value, "gates_per_s": rate.value}
+        cache[key] = {"threads_per_gate": t.value, "gates_per_cta": g.value, "gates_per_s": rate.value}
         tmp = AUTOTUNE_CACHE + ".tmp"
         json.dump(cache, open(tmp, "w"), indent=1)
         os.replace(tmp, AUTOTUNE_CACHE)
-    return g.value, rate.value, False
+    return (t.value, g.value), rate.value, False
 
 
 class Batch:

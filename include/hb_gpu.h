@@ -167,14 +167,16 @@ int hb_external_product_device(hb_ctx *ctx, int field_id, uint32_t log_n, uint32
 
 /* ---- autotuning and mixed-set batches ----------------------------------------------------- */
 
-/* Times every compiled gates-per-CTA variant of the persistent kernel for this key set on
- * sample_gates NAND gates (0: 24 per SM) and keeps the fastest for later launches; reports the
- * choice and its throughput. No counterpart in the reference (its path is single-threaded CPU). */
-int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, int *gates_per_cta,
-                double *gates_per_s);
+/* Times every compiled variant of the persistent kernel for this key set -- threads per gate T
+ * (the NTT tile: 64 threads x 16 words or 128 threads x 8 words, which fixes the device key
+ * layout) and gates per CTA G -- on sample_gates NAND gates (0: 24 per SM), keeps the fastest for
+ * later launches (re-laying the keys out if T changes) and reports it with its throughput.
+ * No counterpart in the reference (its path is single-threaded CPU). */
+int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, int *threads_per_gate,
+                int *gates_per_cta, double *gates_per_s);
 /* Restores a cached autotuner choice; HB_ERR_UNSUPPORTED if that variant is not compiled. */
-int hb_keys_set_gates_per_cta(hb_keys *keys, int gates_per_cta);
-int hb_keys_gates_per_cta(const hb_keys *keys);
+int hb_keys_set_config(hb_ctx *ctx, hb_keys *keys, int threads_per_gate, int gates_per_cta);
+int hb_keys_config(const hb_keys *keys, int *threads_per_gate, int *gates_per_cta);
 
 /* One bootstrapped-gate job of a batch: `count` gates (NAND..MAJORITY) of one key set on device
  * buffers. Batching across gates of the reference's Evaluator (tfhe/src/bfhe/evaluate.rs:113-237). */

@@ -26,13 +26,31 @@ def evaluators(hb, ctx):
         ev.keys.free()
 
 
-def test_autotune_picks_a_compiled_variant(hb, evaluators):
+def test_autotune_picks_a_compiled_variant(hb, evaluators, ctx):
+    import ctypes
     from hasteboots_b200._lib import lib
     sk, ev = evaluators[0]
-    g, rate, cached = hb.autotune(ev, sample_gates=148 * 24, use_cache=False)
-    assert g in (4, 6, 8) and rate > 0
-    assert lib().hb_keys_gates_per_cta(ev.keys.handle) == g
-    assert lib().hb_keys_set_gates_per_cta(ev.keys.handle, 5) != 0  # not compiled
+    (t, g), rate, cached = hb.autotune(ev, sample_gates=148 * 24, use_cache=False)
+    assert t in (64, 128) and g in (4, 6, 8) and rate > 0 and not cached
+    tt, gg = ctypes.c_int(), ctypes.c_int()
+    lib().hb_keys_config(ev.keys.handle, ctypes.byref(tt), ctypes.byref(gg))
+    assert (tt.value, gg.value) == (t, g)
+    assert lib().hb_keys_set_config(ctx.handle, ev.keys.handle, 64, 5) != 0  # not compiled
+
+
+def test_key_relayout_keeps_results(hb, evaluators, ctx):
+    """Switching the NTT tile (threads per gate) re-lays the device keys out; outputs stay identical."""
+    from hasteboots_b200._lib import check, lib
+    for pid in (0, 1):
+        sk, ev = evaluators[pid]
+        bits = np.random.default_rng(9).integers(0, 2, (2, 40)).astype(np.uint8)
+        c0, c1 = sk.encrypt(bits[0], 3000), sk.encrypt(bits[1], 4000)
+        outs = []
+        for t in (64, 128, 64):
+            check(lib().hb_keys_set_config(ctx.handle, ev.keys.handle, t, 4), "set_config", ctx.handle)
+            outs.append(ev.nand(c0, c1))
+        assert (outs[0] == outs[1]).all() and (outs[0] == outs[2]).all()
+        assert (sk.decrypt(outs[1]) == 1 - (bits[0] & bits[1])).all()
 
 
 def test_mixed_batch_equals_alone(hb, evaluators, ctx):
