@@ -464,6 +464,8 @@ def main():
     ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean requests per second")
     ap.add_argument("--drain", type=float, default=30.0, help="serve: seconds to finish after arrivals")
+    ap.add_argument("--variant", default="", help="T,G: use this kernel variant instead of autotuning "
+                                                  "(profiling and sweeps)")
     args = ap.parse_args()
     rank, world, local_rank = dist_env()
     if args.impl == "reference":
@@ -511,7 +513,12 @@ def main():
         check(L.hb_gate_device(ctx.handle, ev.keys.handle, GATE_NAND, d0.data_ptr(), d1.data_ptr(),
                                None, dout.data_ptr(), G), "hb_gate_device", ctx.handle)
 
-    (tuned_t, tuned_g), tuned_rate, tuned_cached = tfhe.autotune(ev)  # setup, outside the timed region
+    if args.variant:
+        tuned_t, tuned_g = (int(x) for x in args.variant.split(","))
+        check(L.hb_keys_set_config(ctx.handle, ev.keys.handle, tuned_t, tuned_g), "set_config", ctx.handle)
+        tuned_rate, tuned_cached = None, None
+    else:  # setup, outside the timed region
+        (tuned_t, tuned_g), tuned_rate, tuned_cached = tfhe.autotune(ev)
     # roofline denominator: measured field-multiplication throughput of this GPU
     probe = ctypes.c_double()
     check(L.hb_probe_modmul(ctx.handle, raw.field_id, ctypes.byref(probe)), "probe", ctx.handle)

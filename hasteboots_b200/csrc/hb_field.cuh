@@ -57,7 +57,13 @@ struct Goldilocks {
 #endif
   }
   // Product with a canonical result.
-  HB_HD static W mul(W a, W b) { return canon(mul_lazy(a, b)); }
+  HB_HD static W mul(W a, W b) {
+#ifdef __CUDA_ARCH__
+    return glx::mul_canon(a, b);
+#else
+    return canon(mul_lazy(a, b));
+#endif
+  }
   // Sum/difference where `b` is canonical (< P): one carry fix-up suffices.
   HB_HD static W add_c(W a, W b) {
     W s = a + b;
@@ -94,7 +100,7 @@ struct Goldilocks {
   // Device hot path: PTX carry-chain arithmetic (hb_gl_ptx.cuh).
   // CT butterfly: (x, y) -> (x + w y, x - w y).
   __device__ __forceinline__ static void ct(W &x, W &y, W w) {
-    const W t = glx::mul(y, w);
+    const W t = glx::mul_canon(y, w);
     const W u = x;
     x = glx::add_c(u, t);
     y = glx::sub_c(u, t);
@@ -106,7 +112,7 @@ struct Goldilocks {
     y = glx::mul_lazy(glx::sub_c(u, v), w);
   }
   // acc += x * k.
-  __device__ __forceinline__ static W mac(W acc, W x, W k) { return glx::add_c(acc, glx::mul(x, k)); }
+  __device__ __forceinline__ static W mac(W acc, W x, W k) { return glx::add_c(acc, glx::mul_canon(x, k)); }
   // First forward stage on words below 2^15 with twiddle 2^48 (the fourth root of unity that the
   // device tables use): x + 2^48 y and x - 2^48 y need no reduction.
   __device__ __forceinline__ static void ct_small_first(W &x, W &y) {

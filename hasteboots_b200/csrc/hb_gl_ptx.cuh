@@ -61,6 +61,51 @@ __device__ __forceinline__ uint64_t mul_lazy(uint64_t a, uint64_t b) {
   return join(r0, r1);
 }
 
+// a * b mod Q, canonical. With the product limbs x0..x3 and A = x2 (2^32 - 1) + (2^32 - 1 - x3)
+// (fits 64 bits), lo + A = r + c 2^64 and a b = r + (c - 1)(2^32 - 1) (mod Q):
+//  * c = 1: r < A <= Q - 1, so r is the canonical result;
+//  * c = 0: r - (2^32 - 1), plus Q when that borrows.
+// Adding c (2^32 - 1) first (on the multiply pipe, it cannot overflow when c = 1) makes both cases
+// one subtraction of 2^32 - 1 with a borrow fix-up.
+__device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
+  uint32_t a0, a1, b0, b1;
+  split(a, a0, a1);
+  split(b, b0, b1);
+  uint32_t x0, x1, x2, x3;
+  asm("mul.lo.u32     %0, %4, %6;\n\t"
+      "mul.hi.u32     %1, %4, %6;\n\t"
+      "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
+      "madc.hi.u32    %2, %4, %7, 0;\n\t"
+      "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "madc.hi.u32    %3, %5, %7, 0;\n\t"
+      "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
+      "addc.u32       %3, %3, 0;"
+      : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  uint64_t A;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  uint32_t A0, A1;
+  split(A, A0, A1);
+  uint32_t r0, r1, c;
+  asm("add.cc.u32  %0, %3, %5;\n\t"
+      "addc.cc.u32 %1, %4, %6;\n\t"
+      "addc.u32    %2, 0, 0;"
+      : "=&r"(r0), "=&r"(r1), "=&r"(c)
+      : "r"(x0), "r"(x1), "r"(A0), "r"(A1));
+  uint64_t r;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(r) : "r"(c), "l"(join(r0, r1)));
+  split(r, r0, r1);
+  asm("{\n\t.reg .u32 bw;\n\t"
+      "sub.cc.u32  %0, %0, 0xFFFFFFFF;\n\t"
+      "subc.cc.u32 %1, %1, 0;\n\t"
+      "subc.u32    bw, 0, 0;\n\t"
+      "sub.cc.u32  %0, %0, bw;\n\t"
+      "subc.u32    %1, %1, 0;\n\t}"
+      : "+r"(r0), "+r"(r1));
+  return join(r0, r1);
+}
+
 // Canonical representative: r >= Q exactly when r + (2^32 - 1) carries out of 64 bits.
 __device__ __forceinline__ uint64_t canon(uint64_t r) {
   uint32_t r0, r1;
