@@ -58,13 +58,19 @@ struct GroupNtt {
   // Slot held by (t, v) at the forward output / inverse input layout.
   __device__ __forceinline__ static int slot_pos(int t, int v) { return t * V + v; }
 
+  // phys is XOR-linear and idx(t, v) = idx(t, 0) ^ (v << LO) (disjoint bits), so
+  // phys(idx(t, v)) = phys(idx(t, 0)) ^ phys(v << LO): a per-thread base and a compile-time constant.
+  __host__ __device__ static constexpr int cphys(int q) { return q ^ ((q >> LOGV) & SWZ); }
+
   template <int LO_FROM, int LO_TO>
   __device__ __forceinline__ static void exchange(W (&x)[V], W *buf, int t, const GroupSync<T> &sync) {
+    const int pf = phys(idx<LO_FROM>(t, 0));
+    const int pt = phys(idx<LO_TO>(t, 0));
 #pragma unroll
-    for (int v = 0; v < V; ++v) buf[phys(idx<LO_FROM>(t, v))] = x[v];
+    for (int v = 0; v < V; ++v) buf[pf ^ cphys(v << LO_FROM)] = x[v];
     sync();
 #pragma unroll
-    for (int v = 0; v < V; ++v) x[v] = buf[phys(idx<LO_TO>(t, v))];
+    for (int v = 0; v < V; ++v) x[v] = buf[pt ^ cphys(v << LO_TO)];
   }
 
   // Twiddle tables are stored stage by stage; within the 2^S entries of a stage, entry
