@@ -16,6 +16,7 @@ gates with its own key copy; no collective on the data path; weak scaling).
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -634,7 +635,7 @@ def main():
                     "frac": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm_peak,
                     "algorithmic_bytes_per_launch": alg_bytes, "peak_source": "MEASURED_PEAKS.json"},
         },
-        "e2e": {"value": G * world / e2e_s, "unit": "bootstraps/s",
+        "e2e": {"value": None if math.isnan(e2e_s) else G * world / e2e_s, "unit": "bootstraps/s",
                 "h2d_bytes_per_step": 2 * G * width * ws, "d2h_bytes_per_step": G * width * ws},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

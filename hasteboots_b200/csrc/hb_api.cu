@@ -120,6 +120,16 @@ int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
     a = hb::host_mulmod<F>(a, psi);
     b = hb::host_mulmod<F>(b, psi_inv);
   }
+  if (F::SMALL_FIRST_GEN) {
+    // The first forward pass multiplies by its twiddles with shifts (GroupNtt::pow2_stage): stages
+    // s <= 4 must hold psi^e = 2^(96 e / N).
+    for (uint32_t s = 0; s <= 4 && s < logn; ++s)
+      for (uint32_t i = 0; i < (1u << s); ++i) {
+        const uint32_t e = brv((1u << s) + i, logn);
+        if ((96ull * e) % N || pw[e] != hb::host_powmod<F>((W)2, (96ull * e) / N))
+          return fail(ctx, HB_ERR_UNSUPPORTED, "twiddle psi^%u is not the expected power of two", e);
+      }
+  }
   for (uint32_t bb = 0; bb < logn; ++bb) {
     // forward stage s = logn-1-bb: blocks i in [0, 2^s), twiddle psi^brv(2^s + i)
     {

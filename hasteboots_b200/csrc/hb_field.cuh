@@ -111,6 +111,14 @@ struct Goldilocks {
     x = glx::add_c(u, v);
     y = glx::mul_lazy(glx::sub_c(u, v), w);
   }
+  // CT butterfly with the twiddle 2^E (compile-time 0 < E < 96): the product comes from shifts.
+  template <int E>
+  __device__ __forceinline__ static void ct_pow2(W &x, W &y) {
+    const W t = glx::mul_pow2<E>(y);
+    const W u = x;
+    x = glx::add_c(u, t);
+    y = glx::sub_c(u, t);
+  }
   // acc += x * k.
   __device__ __forceinline__ static W mac(W acc, W x, W k) { return glx::add_c(acc, glx::mul_canon(x, k)); }
   // First forward stage on words below 2^15 with twiddle 2^48 (the fourth root of unity that the
@@ -135,7 +143,9 @@ struct Goldilocks {
   }
   static W mac(W acc, W x, W k) { return add_c(acc, mul(x, k)); }
 #endif
-  // The device tables pick psi with psi^(2N/64) = 8, so psi^(N/2) = 2^48.
+  // The device tables pick psi with psi^(2N/64) = 8, so psi^(N/2) = 2^48 and every twiddle
+  // psi^e with e a multiple of N/32 is the power of two 2^(96 e / N) (GroupNtt::fwd_stage uses
+  // ct_pow2 for those stages).
   static constexpr uint64_t SMALL_FIRST_GEN = 8;
 };
 

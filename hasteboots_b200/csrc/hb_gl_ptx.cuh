@@ -61,28 +61,14 @@ __device__ __forceinline__ uint64_t mul_lazy(uint64_t a, uint64_t b) {
   return join(r0, r1);
 }
 
-// a * b mod Q, canonical. With the product limbs x0..x3 and A = x2 (2^32 - 1) + (2^32 - 1 - x3)
-// (fits 64 bits), lo + A = r + c 2^64 and a b = r + (c - 1)(2^32 - 1) (mod Q):
+// Canonical residue of the 128-bit value x0 + x1 2^32 + x2 2^64 + x3 2^96 (32-bit limbs). With
+// A = x2 (2^32 - 1) + (2^32 - 1 - x3) (fits 64 bits, A <= 2^64 - 2^32 < Q), lo + A = r + c 2^64 and
+// the value is r + (c - 1)(2^32 - 1) (mod Q):
 //  * c = 1: r < A <= Q - 1, so r is the canonical result;
 //  * c = 0: r - (2^32 - 1), plus Q when that borrows.
 // Adding c (2^32 - 1) first (on the multiply pipe, it cannot overflow when c = 1) makes both cases
 // one subtraction of 2^32 - 1 with a borrow fix-up.
-__device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
-  uint32_t a0, a1, b0, b1;
-  split(a, a0, a1);
-  split(b, b0, b1);
-  uint32_t x0, x1, x2, x3;
-  asm("mul.lo.u32     %0, %4, %6;\n\t"
-      "mul.hi.u32     %1, %4, %6;\n\t"
-      "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
-      "madc.hi.u32    %2, %4, %7, 0;\n\t"
-      "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
-      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
-      "madc.hi.u32    %3, %5, %7, 0;\n\t"
-      "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
-      "addc.u32       %3, %3, 0;"
-      : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
-      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+__device__ __forceinline__ uint64_t reduce_canon(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
   uint64_t A;
   asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
   uint32_t A0, A1;
@@ -104,6 +90,92 @@ __device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
       "subc.u32    %1, %1, 0;\n\t}"
       : "+r"(r0), "+r"(r1));
   return join(r0, r1);
+}
+
+// reduce_canon with x0 = 0: the low limb of lo + A is A0 and cannot carry.
+__device__ __forceinline__ uint64_t reduce_canon_x0zero(uint32_t x1, uint32_t x2, uint32_t x3) {
+  uint64_t A;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  uint32_t A0, A1;
+  split(A, A0, A1);
+  uint32_t r1, c;
+  asm("add.cc.u32  %0, %2, %3;\n\t"
+      "addc.u32    %1, 0, 0;"
+      : "=&r"(r1), "=&r"(c)
+      : "r"(x1), "r"(A1));
+  uint64_t r;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(r) : "r"(c), "l"(join(A0, r1)));
+  uint32_t r0;
+  split(r, r0, r1);
+  asm("{\n\t.reg .u32 bw;\n\t"
+      "sub.cc.u32  %0, %0, 0xFFFFFFFF;\n\t"
+      "subc.cc.u32 %1, %1, 0;\n\t"
+      "subc.u32    bw, 0, 0;\n\t"
+      "sub.cc.u32  %0, %0, bw;\n\t"
+      "subc.u32    %1, %1, 0;\n\t}"
+      : "+r"(r0), "+r"(r1));
+  return join(r0, r1);
+}
+
+// a * b mod Q, canonical: the 128-bit product's limbs, then reduce_canon.
+__device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
+  uint32_t a0, a1, b0, b1;
+  split(a, a0, a1);
+  split(b, b0, b1);
+  uint32_t x0, x1, x2, x3;
+  asm("mul.lo.u32     %0, %4, %6;\n\t"
+      "mul.hi.u32     %1, %4, %6;\n\t"
+      "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
+      "madc.hi.u32    %2, %4, %7, 0;\n\t"
+      "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "madc.hi.u32    %3, %5, %7, 0;\n\t"
+      "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
+      "addc.u32       %3, %3, 0;"
+      : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  return reduce_canon(x0, x1, x2, x3);
+}
+
+// y * 2^E mod Q, canonical, for a compile-time 0 < E < 96 (the twiddles of the first forward
+// stages are such powers of two). The limbs of y 2^E come from shifts instead of multiplies:
+//  * E < 64: y 2^E < 2^128, reduced by reduce_canon;
+//  * E >= 64: y 2^E = z 2^64 + H 2^96 with z = (y 2^(E-64)) mod 2^32 and H = y >> (96 - E), so the
+//    value is z (2^32 - 1) - H. z (2^32 - 1) < Q; when the subtraction borrows, the wrapped word
+//    is at least 2^64 - H and removing one more 2^32 - 1 lands in [0, Q).
+template <int E>
+__device__ __forceinline__ uint64_t mul_pow2(uint64_t y) {
+  static_assert(E > 0 && E < 96, "exponent out of range");
+  uint32_t y0, y1;
+  split(y, y0, y1);
+  if constexpr (E < 32) {
+    return reduce_canon(y0 << E, __funnelshift_l(y0, y1, E), y1 >> (32 - E), 0u);
+  } else if constexpr (E == 32) {
+    return reduce_canon_x0zero(y0, y1, 0u);
+  } else if constexpr (E < 64) {
+    constexpr int e = E - 32;
+    return reduce_canon_x0zero(y0 << e, __funnelshift_l(y0, y1, e), y1 >> (32 - e));
+  } else {
+    constexpr int e = E - 64;
+    const uint32_t z = y0 << e;
+    const uint64_t H = y >> (96 - E);
+    uint32_t h0, h1;
+    split(H, h0, h1);
+    uint64_t A;
+    asm("mul.wide.u32 %0, %1, 0xFFFFFFFF;" : "=l"(A) : "r"(z));
+    uint32_t A0, A1;
+    split(A, A0, A1);
+    uint32_t d0, d1;
+    asm("{\n\t.reg .u32 bw;\n\t"
+        "sub.cc.u32  %0, %2, %4;\n\t"
+        "subc.cc.u32 %1, %3, %5;\n\t"
+        "subc.u32    bw, 0, 0;\n\t"
+        "sub.cc.u32  %0, %0, bw;\n\t"
+        "subc.u32    %1, %1, 0;\n\t}"
+        : "=&r"(d0), "=&r"(d1)
+        : "r"(A0), "r"(A1), "r"(h0), "r"(h1));
+    return join(d0, d1);
+  }
 }
 
 // Canonical representative: r >= Q exactly when r + (2^32 - 1) carries out of 64 bits.

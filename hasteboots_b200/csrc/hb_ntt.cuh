@@ -78,6 +78,35 @@ struct GroupNtt {
   // sits at high + k * (2^S / K), so the loads of a warp are broadcasts or consecutive words
   // (build_tables in hb_api.cu writes this layout).
 
+  __host__ __device__ static constexpr int brvc(int x, int bits) {
+    int r = 0;
+    for (int i = 0; i < bits; ++i) r |= ((x >> i) & 1) << (bits - 1 - i);
+    return r;
+  }
+  // Exponent E with psi^brv(2^S + k) = 2^E when the tables' psi satisfies psi^(N/32) = 8
+  // (brv(2^S + k) is a multiple of N/32 for S <= 4).
+  template <int S, int k>
+  __host__ __device__ static constexpr int pow2_exponent() {
+    return (int)((96LL * brvc((1 << S) + k, LOGN)) >> LOGN);
+  }
+  // Stage S of the first forward pass (layout LO = LOGT, where t >> LO = 0 for every thread): the
+  // k-th twiddle is psi^brv(2^S + k), a compile-time power of two for S <= 4.
+  template <int RB, int S, int k>
+  __device__ __forceinline__ static void pow2_stage(W (&x)[V]) {
+    constexpr int K = V >> (RB + 1);
+    if constexpr (k < K) {
+      static_assert(S >= 0 && S <= 4 && ((96LL * brvc((1 << S) + k, LOGN)) & (N - 1)) == 0,
+                    "twiddle is not a power of two");
+      constexpr int E = pow2_exponent<S, k>();
+#pragma unroll
+      for (int l = 0; l < (1 << RB); ++l) {
+        const int v = (k << (RB + 1)) | l;
+        F::template ct_pow2<E>(x[v], x[v | (1 << RB)]);
+      }
+      pow2_stage<RB, S, k + 1>(x);
+    }
+  }
+
   // One forward (CT) stage on butterfly bit BB in a pass of layout LO. SMALL: inputs are words
   // below 2^15 (gadget digits) and this is the first stage, whose twiddle is 2^48.
   template <int LO, int BB, bool SMALL>
@@ -90,6 +119,8 @@ struct GroupNtt {
 #pragma unroll
       for (int v = 0; v < V; ++v)
         if (!((v >> RB) & 1)) F::ct_small_first(x[v], x[v | (1 << RB)]);
+    } else if constexpr (F::SMALL_FIRST_GEN != 0 && LO == LOGT && S <= 4) {
+      pow2_stage<RB, S, 0>(x);
     } else {
       const int base = (1 << S) + (t >> LO);
 #pragma unroll
