@@ -383,8 +383,9 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
   prm.ks_bits = keys->p.ks_bits;
   prm.status = ctx->d_status;
   prm.budget = wait_budget();
-  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, kStages>;
-  const size_t smem = hb::boot_smem_bytes<W, N, G, kStages>(prm.n);
+  constexpr int S = hb::boot_stages<W, N, G>();
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
+  const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
   const GateJob *djobs = (const GateJob *)ctx->jobs.ptr;
@@ -478,8 +479,9 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
   prm.ks_bits = keys->p.ks_bits;
   prm.status = ctx->d_status;
   prm.budget = wait_budget();
-  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, kStages>;
-  const size_t smem = hb::boot_smem_bytes<W, N, G, kStages>(prm.n);
+  constexpr int S = hb::boot_stages<W, N, G>();
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
+  const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
   grid = std::max(1u, std::min(grid, batches));
@@ -936,8 +938,9 @@ int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJo
   prm.ks_bits = keys->p.ks_bits;
   prm.status = dstatus;
   prm.budget = wait_budget();
-  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, kStages>;
-  const size_t smem = hb::boot_smem_bytes<W, N, G, kStages>(prm.n);
+  constexpr int S = hb::boot_stages<W, N, G>();
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
+  const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
   const unsigned grid = std::min<unsigned>(batches, (unsigned)ctx->sms);

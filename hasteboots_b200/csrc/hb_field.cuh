@@ -121,6 +121,18 @@ struct Goldilocks {
   }
   // acc += x * k.
   __device__ __forceinline__ static W mac(W acc, W x, W k) { return glx::add_c(acc, glx::mul_canon(x, k)); }
+  // Accumulator of a sum of m products, reduced once at the end (glx::mac_lazy).
+  struct Acc {
+    W lo;
+    uint32_t cnt;
+  };
+  __device__ __forceinline__ static void acc_clear(Acc &a) {
+    a.lo = 0;
+    a.cnt = 0;
+  }
+  __device__ __forceinline__ static void acc_mac(Acc &a, W x, W k) { glx::mac_lazy(a.lo, a.cnt, x, k); }
+  // off = acc_offset(m) for an accumulator that took m products.
+  __device__ __forceinline__ static W acc_value(const Acc &a, W off) { return glx::mac_lazy_value(a.lo, a.cnt, off); }
   // First forward stage on words below 2^15 with twiddle 2^48 (the fourth root of unity that the
   // device tables use): x + 2^48 y and x - 2^48 y need no reduction.
   __device__ __forceinline__ static void ct_small_first(W &x, W &y) {
@@ -143,6 +155,7 @@ struct Goldilocks {
   }
   static W mac(W acc, W x, W k) { return add_c(acc, mul(x, k)); }
 #endif
+  HB_HD static W acc_offset(uint32_t products) { return products ? P - (W)products * EPS : 0; }
   // The device tables pick psi with psi^(2N/64) = 8, so psi^(N/2) = 2^48 and every twiddle
   // psi^e with e a multiple of N/32 is the power of two 2^(96 e / N) (GroupNtt::fwd_stage uses
   // ct_pow2 for those stages).
@@ -188,6 +201,14 @@ struct BabyBear {
     y = mont(sub(u, v), w);
   }
   HB_HD static W mac(W acc, W x, W k) { return add(acc, mont(x, k)); }
+  // Accumulator interface shared with Goldilocks: here every product is reduced at once.
+  struct Acc {
+    W w;
+  };
+  HB_HD static void acc_clear(Acc &a) { a.w = 0; }
+  HB_HD static void acc_mac(Acc &a, W x, W k) { a.w = mac(a.w, x, k); }
+  HB_HD static W acc_value(const Acc &a, W) { return a.w; }
+  HB_HD static W acc_offset(uint32_t) { return 0; }
   static constexpr uint64_t SMALL_FIRST_GEN = 0;  // no special first stage
 };
 

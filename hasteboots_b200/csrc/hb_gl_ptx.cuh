@@ -137,6 +137,42 @@ __device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
   return reduce_canon(x0, x1, x2, x3);
 }
 
+// Lazy multiply-accumulate for sums of products: (acc + cnt 2^64) += lo + A, where lo, x2, x3 are
+// the 128-bit product's limbs and A = x2 (2^32 - 1) + (2^32 - 1 - x3), so lo + A = a b + (2^32 - 1)
+// (mod Q) and nothing is reduced per product; cnt counts the carries out of 64 bits. After m calls
+// the sum of the products is acc + cnt (2^32 - 1) - m (2^32 - 1) (mod Q): mac_lazy_value.
+__device__ __forceinline__ void mac_lazy(uint64_t &acc, uint32_t &cnt, uint64_t a, uint64_t b) {
+  uint32_t a0, a1, b0, b1;
+  split(a, a0, a1);
+  split(b, b0, b1);
+  uint32_t x0, x1, x2, x3;
+  asm("mul.lo.u32     %0, %4, %6;\n\t"
+      "mul.hi.u32     %1, %4, %6;\n\t"
+      "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
+      "madc.hi.u32    %2, %4, %7, 0;\n\t"
+      "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
+      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+      "madc.hi.u32    %3, %5, %7, 0;\n\t"
+      "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
+      "addc.u32       %3, %3, 0;"
+      : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
+      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+  uint64_t A;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  uint32_t A0, A1, c0, c1;
+  split(A, A0, A1);
+  split(acc, c0, c1);
+  asm("add.cc.u32  %0, %0, %3;\n\t"
+      "addc.cc.u32 %1, %1, %4;\n\t"
+      "addc.u32    %2, %2, 0;\n\t"
+      "add.cc.u32  %0, %0, %5;\n\t"
+      "addc.cc.u32 %1, %1, %6;\n\t"
+      "addc.u32    %2, %2, 0;"
+      : "+r"(c0), "+r"(c1), "+r"(cnt)
+      : "r"(x0), "r"(x1), "r"(A0), "r"(A1));
+  acc = join(c0, c1);
+}
+
 // y * 2^E mod Q, canonical, for a compile-time 0 < E < 96 (the twiddles of the first forward
 // stages are such powers of two). The limbs of y 2^E come from shifts instead of multiplies:
 //  * E < 64: y 2^E < 2^128, reduced by reduce_canon;
@@ -227,6 +263,15 @@ __device__ __forceinline__ uint64_t sub_c(uint64_t a, uint64_t b) {
       : "=&r"(d0), "=&r"(d1)
       : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
   return join(d0, d1);
+}
+
+// Value of a lazy accumulator as a 64-bit representative: acc + cnt (2^32 - 1) + off, where
+// off = Q - m (2^32 - 1) removes the offsets of the m products (cnt (2^32 - 1) < 2^38 and off < Q,
+// so both additions take the one-carry form).
+__device__ __forceinline__ uint64_t mac_lazy_value(uint64_t acc, uint32_t cnt, uint64_t off) {
+  uint64_t t;
+  asm("mul.wide.u32 %0, %1, 0xFFFFFFFF;" : "=l"(t) : "r"(cnt));
+  return add_c(add_c(acc, t), off);
 }
 
 }  // namespace glx

@@ -333,11 +333,20 @@ struct BootParams {
   long long budget;
 };
 
-// Shared memory words needed by bootstrap_kernel.
+// Shared memory needed by bootstrap_kernel: twiddles (2N words), S key-chunk stages (2N words
+// each), per gate the accumulator (2N), the exchange buffers (2N) and the decomposition source
+// (N), the modulus-switched input (n + 1 halves) and the stage barriers.
 template <class W, int N, int G, int S>
 __host__ __device__ constexpr size_t boot_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(2 * N + S * 2 * N + G * 4 * N) + sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) +
+  return sizeof(W) * (size_t)(2 * N + S * 2 * N + G * 5 * N) + sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) +
          sizeof(uint64_t) * S + 16;
+}
+
+// Key-chunk stages of a bootstrap_kernel variant: 3 when they fit the 227 KB of shared memory a
+// CTA can have (for LWE dimensions up to 1016), else 2.
+template <class W, int N, int G>
+__host__ __device__ constexpr int boot_stages() {
+  return boot_smem_bytes<W, N, G, 3>(1016) <= 232448 ? 3 : 2;
 }
 
 template <class F, int LOGN, int T, int G, int S>
@@ -350,8 +359,9 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   W *s_itw = s_tw + N;
   W *s_k = s_itw + N;
   W *s_grp = s_k + S * 2 * N;
+  W *s_e = s_grp + G * 4 * N;
   const uint32_t msz = (p.n + 8) & ~7u;
-  uint16_t *s_ms = reinterpret_cast<uint16_t *>(s_grp + G * 4 * N);
+  uint16_t *s_ms = reinterpret_cast<uint16_t *>(s_e + G * N);
   uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_ms + G * msz);
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_bar + S);
 
@@ -371,6 +381,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   W *acc_a = s_grp + g * 4 * N;
   W *acc_b = acc_a + N;
   W *xbuf = acc_b + N;
+  W *ebuf = s_e + g * N;  // decomposition source, thread t owns words v * T + t
   uint16_t *ms = s_ms + g * msz;
   int ping = 0;
 
@@ -387,9 +398,11 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   };
   pipe.prime(src);
 
-  const uint64_t br_mask = (1ULL << p.bits) - 1;
-  const uint64_t ks_mask = (1ULL << p.ks_bits) - 1;
   const uint32_t two_n = 2 * N;
+  // Offsets that remove the per-product bookkeeping of the lazy accumulators (F::acc_value): a
+  // blind-rotation step sums 2 len products per slot, the key switch ks_len.
+  const W off_br = F::acc_offset(2 * p.len);
+  const W off_ks = F::acc_offset(p.ks_len);
 
   for (uint32_t batch = blockIdx.x; batch < p.total_batches; batch += gridDim.x) {
     int jx = 0;
@@ -440,9 +453,12 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
     // One loop of 2n + 1 phases shares a single forward-NTT and a single inverse-NTT call site:
     // phase 2i + part decomposes E.a (part 0) or E.b (part 1) of step i, phase 2n decomposes -acc.a
     // for the key switch.
-    W acc_x[V], acc_y[V], e[V];
+    typename F::Acc acc_x[V], acc_y[V];
 #pragma unroll
-    for (int v = 0; v < V; ++v) acc_x[v] = acc_y[v] = 0;
+    for (int v = 0; v < V; ++v) {
+      F::acc_clear(acc_x[v]);
+      F::acc_clear(acc_y[v]);
+    }
     const uint32_t phases = 2 * n + 1;
     for (uint32_t ph = 0; ph < phases; ++ph) {
       const bool ks = ph == 2 * n;
@@ -465,12 +481,12 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             } else {
               rot = y[s + 2 * N];
             }
-            e[v] = F::value(F::sub(rot, y[k]));
+            ebuf[v * T + t] = F::value(F::sub(rot, y[k]));
           }
         } else {
           // sub_assign_gadget_rlwe_mul_polynomial_inplace_fast: p = -acc.a (lattice/src/rlwe.rs:1147-1166)
 #pragma unroll
-          for (int v = 0; v < V; ++v) e[v] = F::value(F::neg_ref(acc_a[NT::natural_pos(t, v)]));
+          for (int v = 0; v < V; ++v) ebuf[v * T + t] = F::value(F::neg_ref(acc_a[NT::natural_pos(t, v)]));
         }
       }
       const uint32_t L = ks ? p.ks_len : p.len;
@@ -481,15 +497,15 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
         if (active) {
           const uint32_t sh = j * bits;
 #pragma unroll
-          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> sh) & mask);
+          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)ebuf[v * T + t] >> sh) & mask);
           NT::forward_small(x, xbuf, ping, s_tw, t, sync);
         }
         const W *k = pipe.acquire();
         if (active) {
 #pragma unroll
           for (int v = 0; v < V; ++v) {
-            acc_x[v] = F::mac(acc_x[v], x[v], k[v * T + t]);
-            acc_y[v] = F::mac(acc_y[v], x[v], k[N + v * T + t]);
+            F::acc_mac(acc_x[v], x[v], k[v * T + t]);
+            F::acc_mac(acc_y[v], x[v], k[N + v * T + t]);
           }
         }
         if (!pipe.release(src)) return;
@@ -497,19 +513,23 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
       if (part == 0 && !ks) continue;
       // Inverse transforms of both accumulators through one call site: h = 0 handles acc_x (the
       // a polynomial), then acc_y moves into acc_x for h = 1 (the b polynomial).
+      const W off = ks ? off_ks : off_br;
       W b0 = 0;
       W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
       if (ks && active) b0 = F::canon(F::add(acc_b[0], (W)(F::P >> 3)));  // evaluate.rs:52
 #pragma unroll 1
       for (int h = 0; h < 2; ++h) {
         if (active) {
-          NT::inverse(acc_x, xbuf, ping, s_itw, t, sync);
+          W f[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) f[v] = F::acc_value(acc_x[v], off);
+          NT::inverse(f, xbuf, ping, s_itw, t, sync);
           if (!ks) {
             W *y = h == 0 ? acc_a : acc_b;
 #pragma unroll
             for (int v = 0; v < V; ++v) {
               const int k = NT::natural_pos(t, v);
-              y[k] = F::add(y[k], F::canon(acc_x[v]));  // RLWE::add_assign_element_wise
+              y[k] = F::add(y[k], F::canon(f[v]));  // RLWE::add_assign_element_wise
             }
           } else {
             // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402): a' = [A0, -A_{N-1}, ...],
@@ -517,7 +537,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
 #pragma unroll
             for (int v = 0; v < V; ++v) {
               const int k = NT::natural_pos(t, v);
-              const W val = F::canon(acc_x[v]);
+              const W val = F::canon(f[v]);
               if (h == 0) {
                 if (k == 0)
                   out[0] = val;
@@ -531,7 +551,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
 #pragma unroll
           for (int v = 0; v < V; ++v) {
             acc_x[v] = acc_y[v];
-            acc_y[v] = 0;
+            F::acc_clear(acc_y[v]);
           }
         }
       }
