@@ -153,6 +153,25 @@ int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
         itw[H + (i % K) * highs + i / K] = F::to_mont(ipw[brv(H + i, logn)]);
     }
   }
+  if (F::RADIX8 && logv == 3) {
+    // Radix-8 passes (GroupNtt::fwd_r8 / inv_r8): every forward pass but the first, and every
+    // inverse pass, that spans three stages holds theta_m^k (theta_m^-k) at 2^S0 + (k-1) 2^S0 + m,
+    // theta_m = psi^brv(2^(S0+2) + 4m) for the 2^S0 blocks of its first stage S0.
+    auto fill = [&](std::vector<W> &tab, uint32_t s0, bool inverse) {
+      const uint32_t blocks = 1u << s0;
+      for (uint32_t m = 0; m < blocks; ++m) {
+        const uint32_t e = brv((1u << (s0 + 2)) + 4 * m, logn);
+        const W th = inverse ? ipw[e] : pw[e];
+        W pk = th;
+        for (uint32_t k = 1; k < 8; ++k) {
+          tab[blocks + (k - 1) * blocks + m] = pk;
+          pk = hb::host_mulmod<F>(pk, th);
+        }
+      }
+    };
+    for (int top = (int)logn - 3; top >= 3; top -= 3) fill(tw, logn - (uint32_t)top, false);
+    for (uint32_t b0 = 0; b0 + 3 <= logn; b0 += 3) fill(itw, logn - 3 - b0, true);
+  }
   const W ninv = hb::host_powmod<F>((W)N, order - 1);
   t.n_inv = F::to_mont(ninv);
   // keys: mul(x, scale) must give x * N^-1 in the Montgomery domain of the key words
@@ -521,7 +540,7 @@ size_t word_size(const hb_params &p) { return p.field_id == HB_FIELD_GOLDILOCKS 
 int default_threads_per_gate(int field_id) {
   const char *env = getenv("HB_THREADS_PER_GATE");
   if (env && (atoi(env) == 64 || atoi(env) == 128)) return atoi(env);
-  return field_id == HB_FIELD_GOLDILOCKS ? 64 : 64;
+  return field_id == HB_FIELD_GOLDILOCKS ? 128 : 64;  // measured best tiles on B200
 }
 
 int default_gates_per_cta(int field_id) {

@@ -111,6 +111,8 @@ struct Goldilocks {
     x = glx::add_c(u, v);
     y = glx::mul_lazy(glx::sub_c(u, v), w);
   }
+  template <int E>
+  __device__ __forceinline__ static W mul_pow2(W y) { return glx::mul_pow2<E>(y); }
   // CT butterfly with the twiddle 2^E (compile-time 0 < E < 96): the product comes from shifts.
   template <int E>
   __device__ __forceinline__ static void ct_pow2(W &x, W &y) {
@@ -160,6 +162,8 @@ struct Goldilocks {
   // psi^e with e a multiple of N/32 is the power of two 2^(96 e / N) (GroupNtt::fwd_stage uses
   // ct_pow2 for those stages).
   static constexpr uint64_t SMALL_FIRST_GEN = 8;
+  // The eighth roots of unity 2^24k make radix-8 passes cheaper than three radix-2 stages.
+  static constexpr bool RADIX8 = true;
 };
 
 struct BabyBear {
@@ -210,6 +214,7 @@ struct BabyBear {
   HB_HD static W acc_value(const Acc &a, W) { return a.w; }
   HB_HD static W acc_offset(uint32_t) { return 0; }
   static constexpr uint64_t SMALL_FIRST_GEN = 0;  // no special first stage
+  static constexpr bool RADIX8 = false;
 };
 
 // Host-side exact helpers used to build tables.

@@ -107,6 +107,78 @@ struct GroupNtt {
     }
   }
 
+  // Radix-8 passes (fields with power-of-two eighth roots of unity, V = 8). The three stages of a
+  // pass act on groups of 8 elements at stride L/8 inside a block of length L whose modulus is
+  // X^L - theta^8, theta = psi^brv(2^(S0+2) + 4m) for block m of the pass's first stage S0. They
+  // equal one pre-multiplication of element k by theta^k (7 products) followed by an 8-point DFT
+  // whose twiddles are the eighth roots of unity 2^24, 2^48, 2^72 (shifts), with the result of
+  // frequency brv3(p) at position p. The inverse pass is the transposed form: an 8-point inverse
+  // DFT on the bit-reversed group, then a post-multiplication by theta^-k. The tables hold theta^k
+  // (theta^-k) at 2^S0 + (k - 1) 2^S0 + m (build_tables in hb_api.cu writes them).
+  static constexpr bool R8 = F::RADIX8 && LOGV == 3;
+  __host__ __device__ static constexpr int brv3(int p) { return ((p & 1) << 2) | (p & 2) | ((p >> 2) & 1); }
+  // (u, v) -> (u + v, u - v) for a canonical v.
+  __device__ __forceinline__ static void bf(W &u, W &v) {
+    const W a = u;
+    u = F::add_c(a, v);
+    v = F::sub_c(a, v);
+  }
+  __device__ __forceinline__ static void bf_canon(W &u, W &v) {
+    v = F::canon(v);
+    bf(u, v);
+  }
+  // (u, v) -> (u - 2^E v, u + 2^E v): the twiddle -2^E = 2^(E + 96).
+  template <int E>
+  __device__ __forceinline__ static void bf_negpow2(W &u, W &v) {
+    const W s = F::template mul_pow2<E>(v);
+    const W a = u;
+    u = F::sub_c(a, s);
+    v = F::add_c(a, s);
+  }
+
+  template <int LO, int S0>
+  __device__ __forceinline__ static void fwd_r8(W (&x)[V], const W *__restrict__ tw, int t) {
+    const W *th = tw + (1 << S0) + (t >> LO);
+    W b[8];
+    b[0] = x[0];
+#pragma unroll
+    for (int p = 1; p < 8; ++p) b[p] = F::mul(x[brv3(p)], th[(brv3(p) - 1) << S0]);
+    // 8-point DFT, decimation in time: bit-reversed input, natural output.
+#pragma unroll
+    for (int i = 0; i < 4; ++i) bf(b[2 * i], b[2 * i + 1]);  // b[odd] are products (canonical)
+#pragma unroll
+    for (int blk = 0; blk < 8; blk += 4) {
+      bf_canon(b[blk], b[blk + 2]);
+      F::template ct_pow2<48>(b[blk + 1], b[blk + 3]);
+    }
+    bf_canon(b[0], b[4]);
+    F::template ct_pow2<24>(b[1], b[5]);
+    F::template ct_pow2<48>(b[2], b[6]);
+    F::template ct_pow2<72>(b[3], b[7]);
+#pragma unroll
+    for (int p = 0; p < 8; ++p) x[p] = b[brv3(p)];
+  }
+
+  template <int LO, int S0>
+  __device__ __forceinline__ static void inv_r8(W (&x)[V], const W *__restrict__ itw, int t) {
+    const W *th = itw + (1 << S0) + (t >> LO);
+    // 8-point inverse DFT (twiddles 2^-24 = -2^72, 2^-48 = -2^48, 2^-72 = -2^24), decimation in
+    // time: the bit-reversed group in, natural order out.
+#pragma unroll
+    for (int i = 0; i < 4; ++i) bf_canon(x[2 * i], x[2 * i + 1]);
+#pragma unroll
+    for (int blk = 0; blk < 8; blk += 4) {
+      bf_canon(x[blk], x[blk + 2]);
+      bf_negpow2<48>(x[blk + 1], x[blk + 3]);
+    }
+    bf_canon(x[0], x[4]);
+    bf_negpow2<72>(x[1], x[5]);
+    bf_negpow2<48>(x[2], x[6]);
+    bf_negpow2<24>(x[3], x[7]);
+#pragma unroll
+    for (int k = 1; k < 8; ++k) x[k] = F::mul(x[k], th[(k - 1) << S0]);
+  }
+
   // One forward (CT) stage on butterfly bit BB in a pass of layout LO. SMALL: inputs are words
   // below 2^15 (gadget digits) and this is the first stage, whose twiddle is 2^48.
   template <int LO, int BB, bool SMALL>
@@ -165,7 +237,10 @@ struct GroupNtt {
   __device__ __forceinline__ static void fwd_pass(W (&x)[V], W *buf, int &ping, const W *tw, int t,
                                                   const GroupSync<T> &sync) {
     constexpr int LO = TOP - LOGV > 0 ? TOP - LOGV : 0;
-    fwd_stages<TOP, TOP - 1, SMALL>(x, tw, t);
+    if constexpr (R8 && TOP < LOGN && TOP - LO == 3)
+      fwd_r8<LO, LOGN - TOP>(x, tw, t);
+    else
+      fwd_stages<TOP, TOP - 1, SMALL>(x, tw, t);
     if constexpr (LO > 0) {
       constexpr int NEXT = LO - LOGV > 0 ? LO - LOGV : 0;
       exchange<LO, NEXT>(x, buf + ping * N, t, sync);
@@ -187,7 +262,10 @@ struct GroupNtt {
                                                   const GroupSync<T> &sync) {
     constexpr int LO = B0 < LOGN - LOGV ? B0 : LOGN - LOGV;
     constexpr int END = B0 + LOGV < LOGN ? B0 + LOGV : LOGN;
-    inv_stages<B0, B0>(x, itw, t);
+    if constexpr (R8 && END - B0 == 3)
+      inv_r8<LO, LOGN - 3 - B0>(x, itw, t);
+    else
+      inv_stages<B0, B0>(x, itw, t);
     if constexpr (END < LOGN) {
       constexpr int NLO = END < LOGN - LOGV ? END : LOGN - LOGV;
       exchange<LO, NLO>(x, buf + ping * N, t, sync);
