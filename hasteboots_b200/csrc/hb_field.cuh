@@ -35,7 +35,13 @@ struct Goldilocks {
   static constexpr int BITS = 64;
   static constexpr int FIELD_ID = 1;
 
-  HB_HD static W canon(W x) { return x >= P ? x - P : x; }
+  HB_HD static W canon(W x) {
+#ifdef __CUDA_ARCH__
+    return glx::canon(x);
+#else
+    return x >= P ? x - P : x;
+#endif
+  }
 
   // Fold a 128-bit value (lo + hi*2^64) to [0, 2^64).
   HB_HD static W fold(W lo, W hi) {
@@ -66,14 +72,22 @@ struct Goldilocks {
   }
   // Sum/difference where `b` is canonical (< P): one carry fix-up suffices.
   HB_HD static W add_c(W a, W b) {
+#ifdef __CUDA_ARCH__
+    return glx::add_c(a, b);
+#else
     W s = a + b;
     if (s < b) s += EPS;
     return s;
+#endif
   }
   HB_HD static W sub_c(W a, W b) {
+#ifdef __CUDA_ARCH__
+    return glx::sub_c(a, b);
+#else
     W d = a - b;
     if (a < b) d -= EPS;
     return d;
+#endif
   }
   // Sum/difference of arbitrary words: the reference's add_reduce / sub_reduce
   // (algebra/src/modulus/goldilocks/ops.rs:26-57).
