@@ -343,7 +343,8 @@ def workload_serve(args):
         ref = ev.nand(p0, p1)
         assert (sk.decrypt(ref) == 1 - (bits[0] & bits[1])).all()
         evs[pid], pools[pid] = (sk, ev), (p0, p1, ref)
-    srv = tfhe.Server(ctx, hbm_budget=120 << 30, max_wave_gates=16384, max_inflight_waves=2)
+    srv = tfhe.Server(ctx, hbm_budget=120 << 30, max_wave_gates=16384, max_inflight_waves=2,
+                      max_queue_s=args.max_queue_s)
     rng = np.random.default_rng(5)
     arrivals, t = [], 0.0
     while True:
@@ -357,6 +358,7 @@ def workload_serve(args):
     meta, lock = {}, threading.Lock()
     mismatches = [0]
     fetched = [0]
+    shed = [0]
     stop_fetch = threading.Event()
 
     def fetcher():
@@ -380,12 +382,15 @@ def workload_serve(args):
             if delay > 0:
                 time.sleep(delay)
             p0, p1, _ = pools[pid]
-            rid = srv.submit(evs[pid][1], "nand", p0[off:off + count], p1[off:off + count])
-            with lock:
+            with lock:  # the fetcher may see the id before submit returns
+                rid = srv.submit(evs[pid][1], "nand", p0[off:off + count], p1[off:off + count])
+                if rid is None:
+                    shed[0] += 1
+                    continue
                 meta[rid] = (pid, off, count)
         submitted_s = time.perf_counter() - t0
         deadline = time.perf_counter() + args.drain
-        while fetched[0] < len(arrivals) and time.perf_counter() < deadline:
+        while fetched[0] < len(arrivals) - shed[0] and time.perf_counter() < deadline:
             time.sleep(0.2)
         st = srv.stats()
     stop_fetch.set()
@@ -399,9 +404,10 @@ def workload_serve(args):
             "config": {"workload": f"Poisson {args.rate} req/s for {args.duration} s, log-uniform 1-4096 NAND "
                                    "gates per request, set uniform over ZAMA/GOLDILOCKS/BABYBEAR",
                        "hbm_budget_gb": 120, "max_wave_gates": 16384, "max_inflight_waves": 2,
-                       "drain_s": args.drain},
+                       "drain_s": args.drain, "max_queue_s": args.max_queue_s},
             "requests": {"submitted": len(arrivals), "completed": int(st["completed"]),
-                         "cancelled_at_stop": len(arrivals) - int(st["completed"]),
+                         "shed": int(st["rejected"]),
+                         "cancelled_at_stop": len(arrivals) - int(st["rejected"]) - int(st["completed"]),
                          "gates_offered": int(sum(a[2] for a in arrivals)),
                          "gates_completed": int(st["gates_completed"]), "waves": int(st["waves"]),
                          "submit_span_s": submitted_s},
@@ -465,6 +471,8 @@ def main():
     ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: mean requests per second")
     ap.add_argument("--drain", type=float, default=30.0, help="serve: seconds to finish after arrivals")
+    ap.add_argument("--max-queue-s", type=float, default=0.0,
+                    help="serve: shed requests predicted to complete later than this (0 = FIFO, admit all)")
     ap.add_argument("--variant", default="", help="T,G: use this kernel variant instead of autotuning "
                                                   "(profiling and sweeps)")
     args = ap.parse_args()

@@ -24,7 +24,7 @@ EXPORTS = [
     "hb_gate", "hb_gate_device", "hb_gate_device_plain", "hb_bootstrap_lut",
     "hb_ntt_forward_device", "hb_ntt_inverse_device", "hb_ntt_roundtrip_device", "hb_rgsw_upload",
     "hb_rgsw_free", "hb_external_product_device", "hb_autotune", "hb_keys_set_config",
-    "hb_keys_config", "hb_batch_create", "hb_batch_launch", "hb_batch_free",
+    "hb_keys_config", "hb_keys_set_rate", "hb_batch_create", "hb_batch_launch", "hb_batch_free",
     "hb_batch_info", "hb_serve_start", "hb_serve_submit", "hb_serve_poll", "hb_serve_next_done",
     "hb_serve_fetch", "hb_serve_stats", "hb_serve_stop", "hb_gate_mux_device_noalloc",
     "hb_probe_modmul", "hb_ctx_launches",
@@ -61,7 +61,7 @@ class HbJob(ctypes.Structure):
 
 class HbServeConfig(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_wave_gates", ctypes.c_uint32),
-                ("max_inflight_waves", ctypes.c_uint32)]
+                ("max_inflight_waves", ctypes.c_uint32), ("max_queue_s", ctypes.c_double)]
 
 
 class HbServeStats(ctypes.Structure):
@@ -69,7 +69,7 @@ class HbServeStats(ctypes.Structure):
                                                 "queued", "waves", "gates_completed")] + \
                [(n, ctypes.c_double) for n in ("p50_latency_s", "p99_latency_s", "mean_latency_s",
                                                 "max_latency_s", "gates_per_s")] + \
-               [("hbm_in_use", ctypes.c_size_t), ("hbm_peak", ctypes.c_size_t)]
+               [("hbm_in_use", ctypes.c_size_t), ("hbm_peak", ctypes.c_size_t), ("rejected", ctypes.c_uint64)]
 
 
 class HbError(RuntimeError):
@@ -126,6 +126,7 @@ def lib():
         "hb_batch_launch": (i32, [vp, vp]),
         "hb_batch_free": (None, [vp, vp]),
         "hb_batch_info": (i32, [vp, ctypes.POINTER(u64), ctypes.POINTER(i32), ctypes.POINTER(i32), i32]),
+        "hb_keys_set_rate": (i32, [vp, ctypes.c_double]),
         "hb_serve_start": (i32, [vp, ctypes.POINTER(HbServeConfig), pp]),
         "hb_serve_submit": (i32, [vp, vp, i32, vp, vp, vp, u32, ctypes.POINTER(u64)]),
         "hb_serve_poll": (i32, [vp, u64, ctypes.POINTER(i32)]),

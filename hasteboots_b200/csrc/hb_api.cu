@@ -1109,6 +1109,12 @@ extern "C" int hb_keys_set_config(hb_ctx *ctx, hb_keys *keys, int threads_per_ga
   return HB_OK;
 }
 
+extern "C" int hb_keys_set_rate(hb_keys *keys, double gates_per_s) {
+  if (!keys || !(gates_per_s >= 0)) return HB_ERR_INVALID;
+  keys->gates_per_s = gates_per_s;
+  return HB_OK;
+}
+
 extern "C" int hb_keys_config(const hb_keys *keys, int *threads_per_gate, int *gates_per_cta) {
   if (!keys) return HB_ERR_INVALID;
   if (threads_per_gate) *threads_per_gate = keys->threads_per_gate;

@@ -10,6 +10,11 @@
 //     wave's CTAs retire (requests that arrive while others run are admitted and overlap on device);
 //  4. marks requests done when their wave's event completes. Outputs stay on the device until the
 //     client fetches them (hb_serve_fetch), which also returns the request's memory to the budget.
+// Optional load shedding (max_queue_s): the server keeps the predicted seconds of work ahead of a
+// new request (sum of count / calibrated gates-per-second of every request not yet completed; the
+// persistent kernels of different key sets share the GPU, so their times add) and refuses a
+// submission that would complete later than max_queue_s from now. Without a bound the queue is
+// FIFO and its latency grows without limit under overload.
 // No counterpart in the reference (its Evaluator is a synchronous single-gate CPU call).
 
 #include <cuda_runtime.h>
@@ -48,6 +53,7 @@ struct Request {
   unsigned char *d_buf = nullptr;
   int state = QUEUED;
   double t_submit = 0, t_done = 0;
+  double work_s = 0;  // predicted GPU seconds (count / calibrated rate), 0 when uncalibrated
 };
 
 struct Wave {
@@ -76,7 +82,8 @@ struct hb_server {
   uint64_t next_id = 1;
   size_t in_use = 0, peak = 0;
   // statistics
-  uint64_t submitted = 0, admitted = 0, completed = 0, failed = 0, waves = 0, gates_done = 0;
+  uint64_t submitted = 0, admitted = 0, completed = 0, failed = 0, waves = 0, gates_done = 0, rejected = 0;
+  double backlog_s = 0;  // predicted seconds of work submitted and not yet completed
   std::vector<double> latencies;
   double t_first_submit = 0, t_last_done = 0;
   // worker-owned CUDA objects
@@ -94,6 +101,7 @@ namespace {
 void fail_request(hb_server *s, Request *r) {
   r->state = FAILED;
   ++s->failed;
+  s->backlog_s = std::max(0.0, s->backlog_s - r->work_s);
   s->done_ids.push_back(r->id);
 }
 
@@ -215,6 +223,7 @@ void complete_waves(hb_server *s) {
         r->state = DONE;
         r->t_done = t;
         ++s->completed;
+        s->backlog_s = std::max(0.0, s->backlog_s - r->work_s);
         s->gates_done += r->count;
         s->latencies.push_back(t - r->t_submit);
         s->t_last_done = t;
@@ -308,6 +317,7 @@ int hb_serve_start(hb_ctx *ctx, const hb_serve_config *cfg, hb_server **out) {
   s->cfg.hbm_budget = cfg && cfg->hbm_budget ? cfg->hbm_budget : (size_t)120 << 30;
   s->cfg.max_wave_gates = cfg ? cfg->max_wave_gates : 0;
   s->cfg.max_inflight_waves = cfg && cfg->max_inflight_waves ? std::min(cfg->max_inflight_waves, 4u) : 2;
+  s->cfg.max_queue_s = cfg && cfg->max_queue_s > 0 ? cfg->max_queue_s : 0;
   cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&s->fetch, cudaStreamNonBlocking);
   s->set_streams.resize(s->cfg.max_inflight_waves * kMaxSets);
@@ -348,6 +358,7 @@ int hb_serve_submit(hb_server *s, hb_keys *keys, int gate, const void *c0, const
   r->lwe_bytes = (size_t)count * (keys->p.lwe_dim + 1) * word_bytes(keys->p);
   r->bytes = (r->nin + 1) * r->lwe_bytes;
   r->t_submit = now_s();
+  if (keys->gates_per_s > 0) r->work_s = count / keys->gates_per_s;
   {
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stopping) {
@@ -358,6 +369,13 @@ int hb_serve_submit(hb_server *s, hb_keys *keys, int gate, const void *c0, const
       delete r;
       return HB_ERR_NOMEM;
     }
+    if (s->cfg.max_queue_s > 0 && r->work_s > 0 && s->backlog_s + r->work_s > s->cfg.max_queue_s) {
+      ++s->rejected;
+      delete r;
+      if (id) *id = 0;
+      return HB_ERR_BUSY;
+    }
+    s->backlog_s += r->work_s;
     r->id = s->next_id++;
     s->reqs[r->id] = r;
     s->queued.push_back(r);
@@ -438,6 +456,7 @@ int hb_serve_stats(hb_server *s, hb_serve_statistics *out) {
   out->gates_completed = s->gates_done;
   out->hbm_in_use = s->in_use;
   out->hbm_peak = s->peak;
+  out->rejected = s->rejected;
   if (!s->latencies.empty()) {
     std::vector<double> l = s->latencies;
     std::sort(l.begin(), l.end());

@@ -313,6 +313,7 @@ def autotune(ev, sample_gates=0, use_cache=True):
         c = cache[key]
         if lib().hb_keys_set_config(ev.ctx.handle, ev.keys.handle, c["threads_per_gate"],
                                     c["gates_per_cta"]) == 0:
+            lib().hb_keys_set_rate(ev.keys.handle, c["gates_per_s"])
             return (c["threads_per_gate"], c["gates_per_cta"]), c["gates_per_s"], True
     t = ctypes.c_int()
     g = ctypes.c_int()
@@ -373,9 +374,9 @@ class Server:
     """Request loop with continuous batching (hb_serve_*). Submissions take host ciphertext arrays
     (pinned memory recommended), which this wrapper keeps alive until fetched."""
 
-    def __init__(self, ctx: Context, hbm_budget=0, max_wave_gates=0, max_inflight_waves=0):
+    def __init__(self, ctx: Context, hbm_budget=0, max_wave_gates=0, max_inflight_waves=0, max_queue_s=0.0):
         from ._lib import HbServeConfig
-        cfg = HbServeConfig(hbm_budget, max_wave_gates, max_inflight_waves)
+        cfg = HbServeConfig(hbm_budget, max_wave_gates, max_inflight_waves, max_queue_s)
         h = ctypes.c_void_p()
         check(lib().hb_serve_start(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)), "hb_serve_start",
               ctx.handle)
@@ -384,10 +385,15 @@ class Server:
         self._live = {}
 
     def submit(self, ev: "Evaluator", gate, c0, c1, c2=None):
+        """Returns the request id, or None when the server refuses the request: its predicted
+        completion lies beyond max_queue_s (load shedding), or the server is stopping."""
         rid = ctypes.c_uint64()
         arrays = [a for a in (c0, c1, c2) if a is not None]
-        check(lib().hb_serve_submit(self.handle, ev.keys.handle, GATE_IDS[gate], _ptr(c0), _ptr(c1),
-                                    _ptr(c2), len(c0), ctypes.byref(rid)), "hb_serve_submit")
+        rc = lib().hb_serve_submit(self.handle, ev.keys.handle, GATE_IDS[gate], _ptr(c0), _ptr(c1),
+                                   _ptr(c2), len(c0), ctypes.byref(rid))
+        if rc == -6 and rid.value == 0:  # HB_ERR_BUSY: refused by the queue-delay bound
+            return None
+        check(rc, "hb_serve_submit")
         self._live[rid.value] = (arrays, ev.params, len(c0))
         return rid.value
 

@@ -177,6 +177,9 @@ int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, int *threads_
 /* Restores a cached autotuner choice; HB_ERR_UNSUPPORTED if that variant is not compiled. */
 int hb_keys_set_config(hb_ctx *ctx, hb_keys *keys, int threads_per_gate, int gates_per_cta);
 int hb_keys_config(const hb_keys *keys, int *threads_per_gate, int *gates_per_cta);
+/* Restores a cached autotuner rate (gates per second of this key set alone), which the serving
+ * loop uses to predict queue delay; hb_autotune sets it. No counterpart in the reference. */
+int hb_keys_set_rate(hb_keys *keys, double gates_per_s);
 
 /* One bootstrapped-gate job of a batch: `count` gates (NAND..MAJORITY) of one key set on device
  * buffers. Batching across gates of the reference's Evaluator (tfhe/src/bfhe/evaluate.rs:113-237). */
@@ -206,12 +209,16 @@ typedef struct hb_serve_config {
   size_t hbm_budget;           /* bytes of request memory (inputs + output) on the device; 0 = 120 GiB */
   uint32_t max_wave_gates;     /* gates packed into one wave at most; 0 = no limit */
   uint32_t max_inflight_waves; /* waves on the GPU at once (1..4); 0 = 2 */
+  double max_queue_s;          /* load shedding: hb_serve_submit refuses (HB_ERR_BUSY) a request whose
+                                  predicted completion, from the work ahead of it and the key sets'
+                                  calibrated rates, lies more than this many seconds away; 0 = admit all */
 } hb_serve_config;
 typedef struct hb_serve_stats {
   uint64_t submitted, admitted, completed, failed, queued, waves, gates_completed;
   double p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s;
   double gates_per_s; /* completed gates / (last completion - first submission) */
   size_t hbm_in_use, hbm_peak;
+  uint64_t rejected; /* submissions refused by the max_queue_s bound */
 } hb_serve_statistics;
 
 /* Starts the request loop of a context (one worker thread). Keys used by requests must outlive it. */

@@ -87,3 +87,31 @@ def test_serve_budget_admits_one_at_a_time(hb, setup):
     st = srv.stats()
     assert st["hbm_peak"] <= largest and st["completed"] == len(reqs)
     assert srv.stop() == 0
+
+
+def test_serve_sheds_load_beyond_queue_bound(hb, setup):
+    """With max_queue_s, a submission whose predicted completion (work ahead of it over the key
+    set's calibrated rate) lies beyond the bound is refused; the admitted ones complete unchanged."""
+    from hasteboots_b200._lib import lib
+    ctx, evs = setup
+    sk, ev = evs[0]
+    assert lib().hb_keys_set_rate(ev.keys.handle, 1000.0) == 0  # 1000 gates/s: 0.2 s per request
+    try:
+        srv = hb.Server(ctx, max_queue_s=0.5)
+        bits = np.random.default_rng(21).integers(0, 2, (2, 200)).astype(np.uint8)
+        c0, c1 = sk.encrypt(bits[0], 77 << 20), sk.encrypt(bits[1], 78 << 20)
+        ids = [srv.submit(ev, "nand", c0, c1) for _ in range(8)]
+        accepted = [i for i in ids if i is not None]
+        assert ids[0] is not None and ids[1] is not None  # 0.4 s of predicted work fits
+        assert len(accepted) < len(ids)
+        ref = ev.nand(c0, c1)
+        for _ in accepted:
+            rid = srv.next_done(60.0)
+            assert rid in accepted
+            out, _ = srv.fetch(rid)
+            assert (out == ref).all()
+        st = srv.stats()
+        assert srv.stop() == 0
+        assert st["rejected"] == len(ids) - len(accepted) and st["completed"] == len(accepted)
+    finally:
+        lib().hb_keys_set_rate(ev.keys.handle, 0.0)
