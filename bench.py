@@ -149,6 +149,7 @@ def cpu_reference(params_id, gates_per_step, steps, warmup, threads):
     c0 = O.encrypt(p, keys.lwe_sk, 0, 0, bits[0])
     c1 = O.encrypt(p, keys.lwe_sk, 0, 1 << 20, bits[1])
     # transform the keys once (Evaluator::new), outside the timed steps
+    keys.evaluator(threads)
     lib = O.lib()
     times = []
     for s in range(warmup + steps):

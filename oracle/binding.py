@@ -71,6 +71,10 @@ def lib():
         L.orc_encrypt.argtypes = [P, vp, u64, u64, vp, sz, vp]
         L.orc_decrypt.argtypes = [P, vp, vp, sz, vp, vp]
         L.orc_gate.argtypes = [P, vp, vp, i32, vp, vp, vp, vp, sz, i32]
+        L.orc_eval_create.argtypes = [P, vp, vp, i32, ctypes.POINTER(vp)]
+        L.orc_eval_free.argtypes = [vp]
+        L.orc_eval_free.restype = None
+        L.orc_eval_gate.argtypes = [vp, i32, vp, vp, vp, vp, sz, i32]
         L.orc_bootstrap_lut.argtypes = [P, vp, vp, vp, vp, vp, sz, i32]
         L.orc_modswitch.argtypes = [P, vp, vp]
         L.orc_blind_rotate.argtypes = [P, vp, vp, vp, ctypes.c_uint32, vp]
@@ -109,6 +113,21 @@ def sizes(p):
 class Keys:
     def __init__(self, p, lwe_sk, ring_sk, bsk, ksk):
         self.p, self.lwe_sk, self.ring_sk, self.bsk, self.ksk = p, lwe_sk, ring_sk, bsk, ksk
+        self._eval = None
+
+    def evaluator(self, threads=None):
+        """Evaluator::new: the keys transformed once (orc_eval_create), reused by every gate."""
+        if self._eval is None:
+            h = ctypes.c_void_p()
+            _check(lib().orc_eval_create(ctypes.byref(self.p), _ptr(self.bsk), _ptr(self.ksk),
+                                         threads or os.cpu_count(), ctypes.byref(h)), "eval_create")
+            self._eval = h
+        return self._eval
+
+    def __del__(self):
+        if getattr(self, "_eval", None) is not None and _lib is not None:
+            _lib.orc_eval_free(self._eval)
+            self._eval = None
 
 
 def keygen(p, seed, threads=None):
@@ -147,9 +166,8 @@ def gate(keys, name, c0, c1=None, c2=None, threads=None):
     c1 = None if c1 is None else np.ascontiguousarray(c1, dtype=dt).reshape(-1, p.lwe_dim + 1)
     c2 = None if c2 is None else np.ascontiguousarray(c2, dtype=dt).reshape(-1, p.lwe_dim + 1)
     out = np.zeros_like(c0)
-    _check(lib().orc_gate(ctypes.byref(p), _ptr(keys.bsk), _ptr(keys.ksk), GATES[name], _ptr(c0),
-                          _ptr(c1), _ptr(c2), _ptr(out), len(c0), threads or os.cpu_count()),
-           "gate")
+    _check(lib().orc_eval_gate(keys.evaluator(threads), GATES[name], _ptr(c0), _ptr(c1), _ptr(c2),
+                               _ptr(out), len(c0), threads or os.cpu_count()), "gate")
     return out
 
 

@@ -35,19 +35,21 @@ struct Gold {
   static constexpr T EPS = 0xFFFFFFFFULL;  // 2^64 mod P
   static constexpr int BITS = 64;          // bits(Q) (algebra/src/goldilocks/mod.rs:69-75)
 
-  static T canon(T x) { return x >= P ? x - P : x; }
+  static T canon(T x) { return x - (P & mask(x >= P)); }
 
-  // 128-bit -> 64-bit folding using 2^64 = 2^32 - 1 and 2^96 = -1 (mod P), written with 128-bit
-  // sums so the compiler emits no data-dependent branches. Result in [0, 2^64), not canonical.
+  // All-ones when c holds: the folds and corrections below are written without data-dependent
+  // branches (about half of them fire on random data).
+  static T mask(bool c) { return (T)0 - (T)c; }
+
+  // 128-bit -> 64-bit folding using 2^64 = 2^32 - 1 and 2^96 = -1 (mod P) (the reduce128 of
+  // algebra/src/modulus/goldilocks/mod.rs:139-150). Result in [0, 2^64), not canonical.
   static T fold128(u128 x) {
-    const T lo = (T)x;
-    const T hi = (T)(x >> 64);
-    const T hh = hi >> 32;
-    const T hl = hi & EPS;
-    u128 t = (u128)lo + (u128)hl * EPS + P - hh;  // x mod P plus P, below 2^66
-    const T tl = (T)t, th = (T)(t >> 64);          // th < 4
-    const u128 r = (u128)tl + (u128)th * EPS;      // below 2^64 + 2^34
-    return (T)r + (T)(r >> 64) * EPS;              // a carry leaves (T)r below 2^34: no overflow
+    const T lo = (T)x, hi = (T)(x >> 64);
+    const T hh = hi >> 32, hl = hi & EPS;
+    const T t0 = lo - hh - (EPS & mask(lo < hh));  // a borrow wraps by 2^64 = P + EPS
+    const T t1 = hl * EPS;
+    const T s = t0 + t1;
+    return s + (EPS & mask(s < t1));  // after a carry s < t1 <= 2^64 - 2^33 + 1: no second carry
   }
 
   // Canonical arithmetic.
@@ -62,6 +64,16 @@ struct Gold {
     return a >= b ? d : d + P;
   }
   static T mul(T a, T b) { return canon(fold128((u128)a * b)); }
+  // Operations on canonical inputs (the transforms keep every word canonical).
+  static T add_cc(T a, T b) {
+    const T s = a + b;
+    return s - (P & mask((s < a) | (s >= P)));
+  }
+  static T sub_cc(T a, T b) { return a - b + (P & mask(a < b)); }
+  // Sum of products reduced once: fold128 values (< 2^64) added in 128 bits.
+  typedef u128 Acc;
+  static void acc_mac(Acc &acc, T a, T b) { acc += fold128((u128)a * b); }
+  static T acc_value(Acc acc) { return canon(fold128(acc)); }
   static T neg(T a) {
     a = canon(a);
     return a == 0 ? 0 : P - a;
@@ -109,6 +121,11 @@ struct Baby {
   }
   static T sub(T a, T b) { return a >= b ? a - b : a + P - b; }
   static T mul(T a, T b) { return (T)(((uint64_t)a * b) % P); }
+  static T add_cc(T a, T b) { return add(a, b); }
+  static T sub_cc(T a, T b) { return sub(a, b); }
+  typedef uint64_t Acc;  // sum of canonical products (each < 2^62), reduced per product
+  static void acc_mac(Acc &acc, T a, T b) { acc += mul(a, b); }
+  static T acc_value(Acc acc) { return (T)(acc % P); }
   static T neg(T a) { return a == 0 ? 0 : P - a; }
   static T add_ref(T a, T b) { return add(a, b); }  // ops.rs:9-17
   static T sub_ref(T a, T b) { return sub(a, b); }  // ops.rs:28-35
@@ -134,16 +151,24 @@ typename F::T finv(typename F::T a) {
 }
 
 // ------------------------------------------------------------------------------------------
-// Negacyclic NTT (plain iterative radix-2, natural order in and out). Slot k holds the
-// evaluation at psi^(2k+1); the constant polynomial c transforms to [c; N], which is the
-// property the reference's key switch initialiser relies on (fhe_core/src/key_switch/rlwe.rs:118-121).
+// Negacyclic NTT: Cooley-Tukey with the psi twist merged into the twiddles (natural order in,
+// bit-reversed slot order out) and the matching Gentleman-Sande inverse (bit-reversed in, natural
+// out, times N^-1). Slot order is internal: every NTT-domain operation on the path is pointwise,
+// and the constant polynomial c still transforms to [c; N], which the reference's key switch
+// initialiser relies on (fhe_core/src/key_switch/rlwe.rs:118-121).
 // ------------------------------------------------------------------------------------------
+
+inline uint32_t bit_reverse(uint32_t x, uint32_t bits) {
+  uint32_t r = 0;
+  for (uint32_t i = 0; i < bits; ++i) r |= ((x >> i) & 1u) << (bits - 1 - i);
+  return r;
+}
 
 template <class F>
 struct Ntt {
   using T = typename F::T;
   uint32_t logn = 0, n = 0;
-  std::vector<T> psi_pow, psi_inv_pow, w_fwd, w_inv;  // w_*: cyclic roots per stage
+  std::vector<T> zeta, izeta;  // zeta[k] = psi^brv(k), izeta[k] = psi^-brv(k), k in [1, n)
   T n_inv = 0;
   bool ok = false;
 
@@ -159,64 +184,55 @@ struct Ntt {
       }
     }
     if (!psi) return;
-    T psi_inv = finv<F>(psi);
-    psi_pow.resize(n);
-    psi_inv_pow.resize(n);
+    const T psi_inv = finv<F>(psi);
+    std::vector<T> pw(n), ipw(n);
     T a = 1, b = 1;
     for (uint32_t i = 0; i < n; ++i) {
-      psi_pow[i] = a;
-      psi_inv_pow[i] = b;
+      pw[i] = a;
+      ipw[i] = b;
       a = F::mul(a, psi);
       b = F::mul(b, psi_inv);
     }
-    T omega = F::mul(psi, psi), omega_inv = F::mul(psi_inv, psi_inv);
-    w_fwd.resize(n);
-    w_inv.resize(n);
-    // w_fwd[len/2 + j] = omega^(j * n/len) for stage of length len
-    for (uint32_t len = 2; len <= n; len <<= 1) {
-      T wl = fpow<F>(omega, n / len), wli = fpow<F>(omega_inv, n / len);
-      T x = 1, y = 1;
-      for (uint32_t j = 0; j < len / 2; ++j) {
-        w_fwd[len / 2 + j] = x;
-        w_inv[len / 2 + j] = y;
-        x = F::mul(x, wl);
-        y = F::mul(y, wli);
-      }
+    zeta.assign(n, 0);
+    izeta.assign(n, 0);
+    for (uint32_t k = 1; k < n; ++k) {
+      zeta[k] = pw[bit_reverse(k, logn)];
+      izeta[k] = ipw[bit_reverse(k, logn)];
     }
     n_inv = finv<F>((T)n);
     ok = true;
   }
 
-  void cyclic(T *a, const std::vector<T> &w) const {
-    for (uint32_t i = 1, j = 0; i < n; ++i) {
-      uint32_t bit = n >> 1;
-      for (; j & bit; bit >>= 1) j ^= bit;
-      j ^= bit;
-      if (i < j) std::swap(a[i], a[j]);
-    }
-    for (uint32_t len = 2; len <= n; len <<= 1) {
-      uint32_t h = len / 2;
-      for (uint32_t i = 0; i < n; i += len) {
-        for (uint32_t j = 0; j < h; ++j) {
-          T u = a[i + j];
-          T v = F::mul(a[i + j + h], w[h + j]);
-          a[i + j] = F::add(u, v);
-          a[i + j + h] = F::sub(u, v);
-        }
-      }
-    }
-  }
-
   // AbstractNTT::transform_slice (algebra/src/transformation/mod.rs:85)
   void forward(T *a) const {
-    for (uint32_t i = 0; i < n; ++i) a[i] = F::mul(F::canon(a[i]), psi_pow[i]);
-    cyclic(a, w_fwd);
+    for (uint32_t i = 0; i < n; ++i) a[i] = F::canon(a[i]);
+    uint32_t k = 1;
+    for (uint32_t len = n >> 1; len >= 1; len >>= 1)
+      for (uint32_t start = 0; start < n; start += 2 * len) {
+        const T w = zeta[k++];
+        for (uint32_t j = start; j < start + len; ++j) {
+          const T t = F::mul(a[j + len], w);
+          const T u = a[j];
+          a[j] = F::add_cc(u, t);
+          a[j + len] = F::sub_cc(u, t);
+        }
+      }
   }
   // AbstractNTT::inverse_transform_slice (algebra/src/transformation/mod.rs:95): inverse + normalize
   void inverse(T *a) const {
     for (uint32_t i = 0; i < n; ++i) a[i] = F::canon(a[i]);
-    cyclic(a, w_inv);
-    for (uint32_t i = 0; i < n; ++i) a[i] = F::mul(F::mul(a[i], n_inv), psi_inv_pow[i]);
+    for (uint32_t len = 1; len < n; len <<= 1) {
+      const uint32_t blocks = n / (2 * len);
+      for (uint32_t blk = 0; blk < blocks; ++blk) {
+        const T w = izeta[blocks + blk];
+        for (uint32_t j = 2 * len * blk; j < 2 * len * blk + len; ++j) {
+          const T u = a[j], v = a[j + len];
+          a[j] = F::add_cc(u, v);
+          a[j + len] = F::mul(F::sub_cc(u, v), w);
+        }
+      }
+    }
+    for (uint32_t i = 0; i < n; ++i) a[i] = F::mul(a[i], n_inv);
   }
 };
 
@@ -583,31 +599,40 @@ template <class F>
 void external_product(const Ntt<F> &ntt, uint32_t bits, uint32_t L, const typename F::T *rgsw_ntt,
                       typename F::T *ea, typename F::T *eb) {
   using T = typename F::T;
+  using Acc = typename F::Acc;
   const uint32_t N = ntt.n;
-  thread_local std::vector<T> ma, mb, poly, digit;
-  ma.assign(N, 0);
-  mb.assign(N, 0);
-  poly.resize(N);
-  digit.resize(N);
+  // Per-thread scratch, addressed through plain pointers inside the loops (a thread_local
+  // object's address is looked up per access in a shared library).
+  thread_local std::vector<T> tl_w;
+  thread_local std::vector<Acc> tl_acc;
+  tl_w.resize((size_t)4 * N);
+  tl_acc.assign((size_t)2 * N, 0);
+  T *ma = tl_w.data(), *mb = ma + N, *poly = mb + N, *digit = poly + N;
+  Acc *sa = tl_acc.data(), *sb = sa + N;
   for (uint32_t part = 0; part < 2; ++part) {
     const T *src = part == 0 ? ea : eb;
-    std::copy(src, src + N, poly.begin());
+    std::copy(src, src + N, poly);
     for (uint32_t j = 0; j < L; ++j) {
-      decompose_step<F>(poly.data(), digit.data(), N, bits);
-      ntt.forward(digit.data());
+      decompose_step<F>(poly, digit, N, bits);
+      ntt.forward(digit);
       const T *ka = rgsw_ntt + ((size_t)part * L + j) * 2 * N;
       const T *kb = ka + N;
-      // ntt_add_mul_assign_fast (algebra/src/polynomial/univariate/ntt_polynomial.rs:620-629)
+      // ntt_add_mul_assign_fast (algebra/src/polynomial/univariate/ntt_polynomial.rs:620-629);
+      // the sums are exact, so reducing once per slot gives the same canonical result
       for (uint32_t k = 0; k < N; ++k) {
-        ma[k] = F::add(ma[k], F::mul(digit[k], ka[k]));
-        mb[k] = F::add(mb[k], F::mul(digit[k], kb[k]));
+        F::acc_mac(sa[k], digit[k], ka[k]);
+        F::acc_mac(sb[k], digit[k], kb[k]);
       }
     }
   }
-  ntt.inverse(ma.data());
-  ntt.inverse(mb.data());
-  std::copy(ma.begin(), ma.end(), ea);
-  std::copy(mb.begin(), mb.end(), eb);
+  for (uint32_t k = 0; k < N; ++k) {
+    ma[k] = F::acc_value(sa[k]);
+    mb[k] = F::acc_value(sb[k]);
+  }
+  ntt.inverse(ma);
+  ntt.inverse(mb);
+  std::copy(ma, ma + N, ea);
+  std::copy(mb, mb + N, eb);
 }
 
 // BinaryBlindRotationKey::blind_rotate (fhe_core/src/blind_rotation/rlwe/binary.rs:28-104).
@@ -870,6 +895,53 @@ int orc_decrypt(const orc_params *p, const void *lwe_sk, const void *lwe, size_t
     for (size_t i = 0; i < count; ++i)
       decrypt<F>(d, (const T *)lwe_sk, (const T *)lwe + i * (d.n + 1),
                  bits_out ? bits_out + i : nullptr, noise_out ? noise_out + i : nullptr);
+  });
+  return 0;
+}
+
+struct orc_eval {
+  orc_params p;
+  Dims d;
+  void *ek;  // EvalKey<Gold> or EvalKey<Baby>
+};
+
+int orc_eval_create(const orc_params *p, const void *bsk, const void *ksk, int threads, orc_eval **out) {
+  Dims d;
+  if (!out || !dims_of(p, d)) return -1;
+  *out = nullptr;
+  ORC_DISPATCH(p, {
+    using T = F::T;
+    orc_eval *e = new orc_eval();
+    e->p = *p;
+    e->d = d;
+    e->ek = make_eval<F>(d, (const T *)bsk, (const T *)ksk, threads);
+    *out = e;
+  });
+  return 0;
+}
+
+void orc_eval_free(orc_eval *e) {
+  if (!e) return;
+  if (e->p.field_id == ORC_FIELD_GOLDILOCKS)
+    delete (EvalKey<Gold> *)e->ek;
+  else
+    delete (EvalKey<Baby> *)e->ek;
+  delete e;
+}
+
+int orc_eval_gate(const orc_eval *e, int gate, const void *c0, const void *c1, const void *c2,
+                  void *out, size_t count, int threads) {
+  if (!e || gate < 0 || gate > ORC_GATE_MUX) return -1;
+  if ((gate == ORC_GATE_MAJORITY || gate == ORC_GATE_MUX) && !c2) return -1;
+  const Dims &d = e->d;
+  ORC_DISPATCH(&e->p, {
+    using T = F::T;
+    const EvalKey<F> &ek = *(const EvalKey<F> *)e->ek;
+    const size_t m = d.n + 1;
+    parallel_for(count, threads, [&](size_t i) {
+      gate_one<F>(ek, gate, (const T *)c0 + i * m, c1 ? (const T *)c1 + i * m : nullptr,
+                  c2 ? (const T *)c2 + i * m : nullptr, (T *)out + i * m);
+    });
   });
   return 0;
 }

@@ -84,6 +84,15 @@ int orc_decrypt(const orc_params *p, const void *lwe_sk, const void *lwe, size_t
 int orc_gate(const orc_params *p, const void *bsk, const void *ksk, int gate, const void *c0,
              const void *c1, const void *c2, void *out, size_t count, int threads);
 
+/* Evaluator::new (tfhe/src/bfhe/evaluate.rs:65-96): the bootstrapping and key-switching keys
+ * transformed once into an opaque handle, so that gates on it skip the key transform. */
+typedef struct orc_eval orc_eval;
+int orc_eval_create(const orc_params *p, const void *bsk, const void *ksk, int threads, orc_eval **out);
+void orc_eval_free(orc_eval *e);
+/* orc_gate on a transformed key. */
+int orc_eval_gate(const orc_eval *e, int gate, const void *c0, const void *c1, const void *c2,
+                  void *out, size_t count, int threads);
+
 /* EvaluationKey::bootstrap(c, lut) on count ciphertexts sharing one LUT polynomial (N words). */
 int orc_bootstrap_lut(const orc_params *p, const void *bsk, const void *ksk, const void *c,
                       const void *lut, void *out, size_t count, int threads);
