@@ -73,22 +73,22 @@ __device__ __forceinline__ uint64_t reduce_canon(uint32_t x0, uint32_t x1, uint3
   asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
   uint32_t A0, A1;
   split(A, A0, A1);
-  uint32_t r0, r1, c;
-  asm("add.cc.u32  %0, %3, %5;\n\t"
-      "addc.cc.u32 %1, %4, %6;\n\t"
-      "addc.u32    %2, 0, 0;"
-      : "=&r"(r0), "=&r"(r1), "=&r"(c)
+  uint32_t r0, r1;
+  // r + c (2^32 - 1) on 32-bit halves (c (2^32 - 1) has high word 0, so the high half only takes
+  // the carry), then the subtraction of 2^32 - 1 with its borrow fix-up.
+  asm("{\n\t.reg .u32 c, bw;\n\t"
+      "add.cc.u32     %0, %2, %4;\n\t"
+      "addc.cc.u32    %1, %3, %5;\n\t"
+      "addc.u32       c, 0, 0;\n\t"
+      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %0;\n\t"
+      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t"
+      "sub.cc.u32     %0, %0, 0xFFFFFFFF;\n\t"
+      "subc.cc.u32    %1, %1, 0;\n\t"
+      "subc.u32       bw, 0, 0;\n\t"
+      "sub.cc.u32     %0, %0, bw;\n\t"
+      "subc.u32       %1, %1, 0;\n\t}"
+      : "=&r"(r0), "=&r"(r1)
       : "r"(x0), "r"(x1), "r"(A0), "r"(A1));
-  uint64_t r;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(r) : "r"(c), "l"(join(r0, r1)));
-  split(r, r0, r1);
-  asm("{\n\t.reg .u32 bw;\n\t"
-      "sub.cc.u32  %0, %0, 0xFFFFFFFF;\n\t"
-      "subc.cc.u32 %1, %1, 0;\n\t"
-      "subc.u32    bw, 0, 0;\n\t"
-      "sub.cc.u32  %0, %0, bw;\n\t"
-      "subc.u32    %1, %1, 0;\n\t}"
-      : "+r"(r0), "+r"(r1));
   return join(r0, r1);
 }
 
@@ -98,22 +98,19 @@ __device__ __forceinline__ uint64_t reduce_canon_x0zero(uint32_t x1, uint32_t x2
   asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
   uint32_t A0, A1;
   split(A, A0, A1);
-  uint32_t r1, c;
-  asm("add.cc.u32  %0, %2, %3;\n\t"
-      "addc.u32    %1, 0, 0;"
-      : "=&r"(r1), "=&r"(c)
-      : "r"(x1), "r"(A1));
-  uint64_t r;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(r) : "r"(c), "l"(join(A0, r1)));
-  uint32_t r0;
-  split(r, r0, r1);
-  asm("{\n\t.reg .u32 bw;\n\t"
-      "sub.cc.u32  %0, %0, 0xFFFFFFFF;\n\t"
-      "subc.cc.u32 %1, %1, 0;\n\t"
-      "subc.u32    bw, 0, 0;\n\t"
-      "sub.cc.u32  %0, %0, bw;\n\t"
-      "subc.u32    %1, %1, 0;\n\t}"
-      : "+r"(r0), "+r"(r1));
+  uint32_t r0, r1;
+  asm("{\n\t.reg .u32 c, bw;\n\t"
+      "add.cc.u32     %1, %2, %3;\n\t"
+      "addc.u32       c, 0, 0;\n\t"
+      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %4;\n\t"
+      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t"
+      "sub.cc.u32     %0, %0, 0xFFFFFFFF;\n\t"
+      "subc.cc.u32    %1, %1, 0;\n\t"
+      "subc.u32       bw, 0, 0;\n\t"
+      "sub.cc.u32     %0, %0, bw;\n\t"
+      "subc.u32       %1, %1, 0;\n\t}"
+      : "=&r"(r0), "=&r"(r1)
+      : "r"(x1), "r"(A1), "r"(A0));
   return join(r0, r1);
 }
 
@@ -218,16 +215,14 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t y) {
 __device__ __forceinline__ uint64_t canon(uint64_t r) {
   uint32_t r0, r1;
   split(r, r0, r1);
-  uint32_t c;
-  asm("{\n\t.reg .u32 t0, t1;\n\t"
-      "add.cc.u32  t0, %1, 0xFFFFFFFF;\n\t"
-      "addc.cc.u32 t1, %2, 0;\n\t"
-      "addc.u32    %0, 0, 0;\n\t}"
-      : "=r"(c)
-      : "r"(r0), "r"(r1));
-  uint64_t out;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(out) : "r"(c), "l"(r));
-  return out;
+  asm("{\n\t.reg .u32 t0, t1, c;\n\t"
+      "add.cc.u32     t0, %0, 0xFFFFFFFF;\n\t"
+      "addc.cc.u32    t1, %1, 0;\n\t"
+      "addc.u32       c, 0, 0;\n\t"
+      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %0;\n\t"
+      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t}"
+      : "+r"(r0), "+r"(r1));
+  return join(r0, r1);
 }
 
 __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) { return canon(mul_lazy(a, b)); }
@@ -237,15 +232,16 @@ __device__ __forceinline__ uint64_t add_c(uint64_t a, uint64_t b) {
   uint32_t a0, a1, b0, b1;
   split(a, a0, a1);
   split(b, b0, b1);
-  uint32_t s0, s1, c;
-  asm("add.cc.u32  %0, %3, %5;\n\t"
-      "addc.cc.u32 %1, %4, %6;\n\t"
-      "addc.u32    %2, 0, 0;"
-      : "=&r"(s0), "=&r"(s1), "=&r"(c)
+  uint32_t s0, s1;
+  asm("{\n\t.reg .u32 c;\n\t"
+      "add.cc.u32     %0, %2, %4;\n\t"
+      "addc.cc.u32    %1, %3, %5;\n\t"
+      "addc.u32       c, 0, 0;\n\t"
+      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %0;\n\t"
+      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t}"
+      : "=&r"(s0), "=&r"(s1)
       : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-  uint64_t out;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(out) : "r"(c), "l"(join(s0, s1)));
-  return out;
+  return join(s0, s1);
 }
 
 // a - b with b < Q: at most one borrow, worth -(2^32 - 1), and removing it cannot borrow again.
