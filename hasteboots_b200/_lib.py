@@ -8,7 +8,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhb_gpu.so")
+# HB_GPU_LIB selects another build of the same library (for example one with different build flags).
+LIB_PATH = os.environ.get("HB_GPU_LIB") or os.path.join(HERE, "libhb_gpu.so")
 
 HB_OK = 0
 ERRORS = {-1: "HB_ERR_INVALID", -2: "HB_ERR_CUDA", -3: "HB_ERR_NOMEM", -4: "HB_ERR_TIMEOUT",

@@ -114,24 +114,12 @@ __device__ __forceinline__ uint64_t reduce_canon_x0zero(uint32_t x1, uint32_t x2
   return join(r0, r1);
 }
 
-// a * b mod Q, canonical: the 128-bit product's limbs, then reduce_canon.
+// a * b mod Q, canonical: the 128-bit product's limbs, then reduce_canon. The product is left to
+// the compiler's 64-bit multiply lowering (measured faster here than a hand-written chain of
+// 32-bit mad.lo.cc / madc.hi.cc, whose single carry flag serialises it).
 __device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
-  uint32_t a0, a1, b0, b1;
-  split(a, a0, a1);
-  split(b, b0, b1);
-  uint32_t x0, x1, x2, x3;
-  asm("mul.lo.u32     %0, %4, %6;\n\t"
-      "mul.hi.u32     %1, %4, %6;\n\t"
-      "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
-      "madc.hi.u32    %2, %4, %7, 0;\n\t"
-      "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
-      "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
-      "madc.hi.u32    %3, %5, %7, 0;\n\t"
-      "mad.lo.cc.u32  %2, %5, %7, %2;\n\t"
-      "addc.u32       %3, %3, 0;"
-      : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
-      : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-  return reduce_canon(x0, x1, x2, x3);
+  const uint64_t lo = a * b, hi = __umul64hi(a, b);
+  return reduce_canon((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
 }
 
 // Lazy multiply-accumulate for sums of products: (acc + cnt 2^64) += lo + A, where lo, x2, x3 are

@@ -315,6 +315,29 @@ __global__ void __launch_bounds__(G * T, 1)
   }
 }
 
+// Digit j of the unsigned LSB-first decomposition (Polynomial::decompose_lsb_bits_inplace,
+// algebra/src/polynomial/univariate/native_polynomial.rs:340-348) of the words e[v * T + t]:
+// (e >> sh) & mask with sh = j * bits uniform, as one funnel shift of the word's halves (or one
+// shift of the high half) and a mask.
+template <class W, int V, int T>
+__device__ __forceinline__ void digits(W (&x)[V], const W *e, int t, uint32_t sh, uint32_t mask) {
+  if constexpr (sizeof(W) == 8) {
+    if (sh < 32) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const uint64_t w = e[v * T + t];
+        x[v] = __funnelshift_r((uint32_t)w, (uint32_t)(w >> 32), sh) & mask;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) x[v] = ((uint32_t)(e[v * T + t] >> 32) >> (sh - 32)) & mask;
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < V; ++v) x[v] = (e[v * T + t] >> sh) & mask;
+  }
+}
+
 // ------------------------------------------------------------------------------------------
 // Persistent batched bootstrapping (EvaluationKey::bootstrap, tfhe/src/bfhe/evaluate.rs:42-60)
 // ------------------------------------------------------------------------------------------
@@ -496,8 +519,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
         W x[V];
         if (active) {
           const uint32_t sh = j * bits;
-#pragma unroll
-          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)ebuf[v * T + t] >> sh) & mask);
+          digits<W, V, T>(x, ebuf, t, sh, (uint32_t)mask);
           NT::forward_small(x, xbuf, ping, s_tw, t, sync);
         }
         const W *k = pipe.acquire();
