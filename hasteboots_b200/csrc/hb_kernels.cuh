@@ -121,6 +121,73 @@ struct ChunkPipe {
   }
 };
 
+// The same ring consumed by G independent thread groups without a CTA-wide barrier: each group
+// releases a stage after its own barrier by counting itself in `cnt`; the group whose count
+// completes a multiple of G refills the stage. Groups can therefore drift up to S - 1 chunks apart (one may run
+// its multiply-heavy accumulate while another runs the add-heavy transform). `issued` counts the
+// copies per stage so that an aborting CTA can wait for the ones in flight.
+template <class W, int N, int S, int G>
+struct GroupPipe {
+  W *stages;
+  uint64_t *bars;
+  uint32_t *cnt, *issued;
+  volatile int *abort_flag;
+  int *status;
+  long long budget;
+  unsigned long long next;
+  unsigned long long total;
+  static constexpr uint32_t WORDS = 2 * N;
+  static constexpr uint32_t BYTES = WORDS * sizeof(W);
+
+  template <class Src>
+  __device__ __forceinline__ void prime(const Src &src) {
+    if (threadIdx.x == 0)
+      for (unsigned long long c = 0; c < (unsigned long long)S && c < total; ++c) {
+        issued[c] = 1;
+        mbar_arrive_expect_tx(&bars[c], BYTES);
+        bulk_g2s(stages + c * WORDS, src(c), BYTES, &bars[c]);
+      }
+  }
+  __device__ __forceinline__ const W *acquire() {
+    const int st = (int)(next % S);
+    const uint32_t par = (uint32_t)((next / S) & 1);
+    if (!mbar_wait_bounded(&bars[st], par, budget)) {
+      *abort_flag = 1;
+      atomicOr(status, STATUS_TIMEOUT);
+    }
+    return stages + st * WORDS;
+  }
+  // Group-wide release of the current chunk (t: the thread's index in its group); false when the
+  // launch must stop.
+  template <class Src, class Sync>
+  __device__ __forceinline__ bool release(const Src &src, int t, const Sync &sync) {
+    sync();  // every thread of this group is done reading the stage
+    if (*abort_flag) return false;
+    if (t == 0) {
+      const int st = (int)(next % S);
+      __threadfence_block();
+      if ((atomicAdd(&cnt[st], 1u) + 1) % G == 0) {  // counts only grow: no reset to order
+        __threadfence_block();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (next + S < total) {
+          issued[st] += 1;
+          mbar_arrive_expect_tx(&bars[st], BYTES);
+          bulk_g2s(stages + st * WORDS, src(next + S), BYTES, &bars[st]);
+        }
+      }
+    }
+    ++next;
+    return true;
+  }
+  // After an abort, with every thread of the CTA past its loops: wait (bounded) for the last copy
+  // issued into each stage.
+  __device__ __forceinline__ void drain() {
+    if (threadIdx.x != 0) return;
+    for (int st = 0; st < S; ++st)
+      if (issued[st]) mbar_wait_bounded(&bars[st], (issued[st] - 1) & 1, budget);
+  }
+};
+
 // ------------------------------------------------------------------------------------------
 // Key preparation
 // ------------------------------------------------------------------------------------------
@@ -362,7 +429,7 @@ struct BootParams {
 template <class W, int N, int G, int S>
 __host__ __device__ constexpr size_t boot_smem_bytes(uint32_t n) {
   return sizeof(W) * (size_t)(2 * N + S * 2 * N + G * 5 * N) + sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) +
-         sizeof(uint64_t) * S + 16;
+         sizeof(uint64_t) * S + 2 * sizeof(uint32_t) * S + 16;
 }
 
 // Key-chunk stages of a bootstrap_kernel variant: 3 when they fit the 227 KB of shared memory a
@@ -386,7 +453,9 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   const uint32_t msz = (p.n + 8) & ~7u;
   uint16_t *s_ms = reinterpret_cast<uint16_t *>(s_e + G * N);
   uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_ms + G * msz);
-  volatile int *s_abort = reinterpret_cast<volatile int *>(s_bar + S);
+  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_bar + S);
+  uint32_t *s_issued = s_cnt + S;
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_issued + S);
 
   const int tid = threadIdx.x, g = tid / T, t = tid % T;
   for (int i = tid; i < N; i += blockDim.x) {
@@ -394,7 +463,11 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
     s_itw[i] = p.itw[i];
   }
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&s_bar[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&s_bar[s], 1);
+      s_cnt[s] = 0;
+      s_issued[s] = 0;
+    }
     mbar_fence_init();
     *s_abort = 0;
   }
@@ -413,8 +486,8 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   const uint32_t cpb = br_chunks + p.ks_len;
   const uint32_t my_batches =
       blockIdx.x < p.total_batches ? (p.total_batches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  ChunkPipe<W, N, S> pipe{s_k, s_bar, s_abort, p.status, p.budget, 0,
-                          (unsigned long long)my_batches * cpb};
+  GroupPipe<W, N, S, G> pipe{s_k, s_bar, s_cnt, s_issued, s_abort, p.status, p.budget, 0,
+                             (unsigned long long)my_batches * cpb};
   auto src = [&](unsigned long long c) -> const W * {
     const uint32_t q = (uint32_t)(c % cpb);
     return q < br_chunks ? p.bsk + (size_t)q * 2 * N : p.ksk + (size_t)(q - br_chunks) * 2 * N;
@@ -530,7 +603,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             F::acc_mac(acc_y[v], x[v], k[N + v * T + t]);
           }
         }
-        if (!pipe.release(src)) return;
+        if (!pipe.release(src, t, sync)) goto aborted;
       }
       if (part == 0 && !ks) continue;
       // Inverse transforms of both accumulators through one call site: h = 0 handles acc_x (the
@@ -580,6 +653,12 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
       sync();
     }
   }
+
+  // Every thread ends here, including the groups that stopped on an abort, so that copies still
+  // in flight into shared memory are waited for before the CTA exits.
+aborted:
+  __syncthreads();
+  if (*s_abort) pipe.drain();
 }
 
 // ------------------------------------------------------------------------------------------
