@@ -28,7 +28,7 @@ EXPORTS = [
     "hb_keys_config", "hb_keys_set_rate", "hb_batch_create", "hb_batch_launch", "hb_batch_free",
     "hb_batch_info", "hb_serve_start", "hb_serve_submit", "hb_serve_poll", "hb_serve_next_done",
     "hb_serve_fetch", "hb_serve_stats", "hb_serve_stop", "hb_gate_mux_device_noalloc",
-    "hb_probe_modmul", "hb_ctx_launches",
+    "hb_probe_modmul", "hb_ctx_launches", "hb_ctx_set_wait_limit", "hb_ctx_test_withhold_keys",
 ]
 
 
@@ -138,6 +138,8 @@ def lib():
         "hb_gate_mux_device_noalloc": (i32, [vp, vp, vp, vp, vp, vp, sz]),
         "hb_probe_modmul": (i32, [vp, i32, ctypes.POINTER(ctypes.c_double)]),
         "hb_ctx_launches": (u64, [vp]),
+        "hb_ctx_set_wait_limit": (i32, [vp, ctypes.c_longlong]),
+        "hb_ctx_test_withhold_keys": (i32, [vp, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -218,7 +218,8 @@ int check_status(hb_ctx *ctx) {
   return HB_OK;
 }
 
-long long wait_budget() { return 4000000000LL; }  // ~2 s of SM clocks per bounded wait
+// ~2 s of SM clocks per bounded wait unless the context sets another limit (hb_ctx_set_wait_limit)
+long long wait_budget(const hb_ctx *ctx) { return ctx && ctx->wait_limit > 0 ? ctx->wait_limit : 4000000000LL; }
 
 }  // namespace hbrt
 
@@ -314,7 +315,7 @@ int launch_ext(hb_ctx *ctx, const void *rgsw, uint32_t bits, uint32_t len, const
   const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(batches, (size_t)ctx->sms));
   kern<<<grid, G * T, smem, ctx->stream>>>((const W *)in, (W *)out, count, (const W *)rgsw, len, bits,
                                             (const W *)tb->tw, (const W *)tb->itw, ctx->d_status,
-                                            wait_budget());
+                                            wait_budget(ctx));
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? HB_OK : cuda_fail(ctx, e, "external product launch");
 }
@@ -401,7 +402,8 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
   prm.ks_len = keys->p.ks_len;
   prm.ks_bits = keys->p.ks_bits;
   prm.status = ctx->d_status;
-  prm.budget = wait_budget();
+  prm.budget = wait_budget(ctx);
+  prm.withhold = ctx->withhold_keys;
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
@@ -497,7 +499,8 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
   prm.ks_len = keys->p.ks_len;
   prm.ks_bits = keys->p.ks_bits;
   prm.status = ctx->d_status;
-  prm.budget = wait_budget();
+  prm.budget = wait_budget(ctx);
+  prm.withhold = ctx->withhold_keys;
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
@@ -899,6 +902,18 @@ int hb_probe_modmul(hb_ctx *ctx, int field_id, double *modmul_per_s) {
 
 uint64_t hb_ctx_launches(const hb_ctx *ctx) { return ctx ? ctx->launches.load() : 0; }
 
+int hb_ctx_set_wait_limit(hb_ctx *ctx, long long clock_cycles) {
+  if (!ctx || clock_cycles < 0) return HB_ERR_INVALID;
+  ctx->wait_limit = clock_cycles;
+  return HB_OK;
+}
+
+int hb_ctx_test_withhold_keys(hb_ctx *ctx, int on) {
+  if (!ctx) return HB_ERR_INVALID;
+  ctx->withhold_keys = on ? 1 : 0;
+  return HB_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------
@@ -956,7 +971,7 @@ int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJo
   prm.ks_len = keys->p.ks_len;
   prm.ks_bits = keys->p.ks_bits;
   prm.status = dstatus;
-  prm.budget = wait_budget();
+  prm.budget = wait_budget(ctx);
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);

@@ -19,6 +19,10 @@ namespace hb {
 
 enum : int { STATUS_OK = 0, STATUS_TIMEOUT = 1 };
 
+// Clock budget of the wait, on an abort, for bulk copies still in flight into shared memory. It is
+// independent of the launch's wait limit: a CTA must not exit while a copy can still land.
+constexpr long long kDrainBudget = 4000000000LL;
+
 // ------------------------------------------------------------------------------------------
 // Shared pieces
 // ------------------------------------------------------------------------------------------
@@ -117,7 +121,7 @@ struct ChunkPipe {
   __device__ __forceinline__ void drain() {
     if (threadIdx.x != 0) return;
     for (unsigned long long c = next; c < next + S && c < total; ++c)
-      mbar_wait_bounded(&bars[c % S], (uint32_t)((c / S) & 1), budget);
+      mbar_wait_bounded(&bars[c % S], (uint32_t)((c / S) & 1), kDrainBudget);
   }
 };
 
@@ -184,7 +188,7 @@ struct GroupPipe {
   __device__ __forceinline__ void drain() {
     if (threadIdx.x != 0) return;
     for (int st = 0; st < S; ++st)
-      if (issued[st]) mbar_wait_bounded(&bars[st], (issued[st] - 1) & 1, budget);
+      if (issued[st]) mbar_wait_bounded(&bars[st], (issued[st] - 1) & 1, kDrainBudget);
   }
 };
 
@@ -421,6 +425,7 @@ struct BootParams {
   uint32_t n, len, bits, ks_len, ks_bits;
   int *status;
   long long budget;
+  int withhold;  // test hook: issue no key-chunk copy, so the first wait runs out (bounded)
 };
 
 // Shared memory needed by bootstrap_kernel: twiddles (2N words), S key-chunk stages (2N words
@@ -487,7 +492,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   const uint32_t my_batches =
       blockIdx.x < p.total_batches ? (p.total_batches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   GroupPipe<W, N, S, G> pipe{s_k, s_bar, s_cnt, s_issued, s_abort, p.status, p.budget, 0,
-                             (unsigned long long)my_batches * cpb};
+                             p.withhold ? 0ull : (unsigned long long)my_batches * cpb};
   auto src = [&](unsigned long long c) -> const W * {
     const uint32_t q = (uint32_t)(c % cpb);
     return q < br_chunks ? p.bsk + (size_t)q * 2 * N : p.ksk + (size_t)(q - br_chunks) * 2 * N;

@@ -42,6 +42,8 @@ struct hb_ctx {
   hbrt::DevTables tables[2][13][6];  // [field][log2 N][log2 words per thread]
   hbrt::Scratch jobs, io, mux_tmp, acc;
   std::atomic<unsigned long long> launches{0};  // bootstrap kernel launches issued by this context
+  long long wait_limit = 0;                     // SM clock cycles per bounded wait; 0 = default
+  int withhold_keys = 0;                        // test hook: bootstrap launches issue no key copies
 };
 
 struct hb_keys {
@@ -62,7 +64,7 @@ void dev_free(hb_ctx *ctx, void *p);
 int scratch(hb_ctx *ctx, Scratch &s, size_t bytes);
 int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out, uint32_t logv = 4);
 int check_status(hb_ctx *ctx);
-long long wait_budget();
+long long wait_budget(const hb_ctx *ctx);
 // One persistent bootstrapping launch over a device job table (full grid, the keys' variant).
 int launch_set(hb_ctx *ctx, hb_keys *keys, const hb::GateJob *djobs, int njobs, uint32_t batches,
                cudaStream_t stream);

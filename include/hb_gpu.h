@@ -261,6 +261,15 @@ int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void *c0, const
 int hb_probe_modmul(hb_ctx *ctx, int field_id, double *modmul_per_s);
 /* Kernel launches the context has issued for bootstrapping (batched and plain forms). */
 uint64_t hb_ctx_launches(const hb_ctx *ctx);
+/* Limit, in SM clock cycles, of every bounded wait inside this context's kernels (waits for key
+ * chunks in flight); 0 restores the default (about 2 s). A wait that runs out makes the call return
+ * HB_ERR_TIMEOUT and leaves the context usable; tests use a tiny limit to exercise that path.
+ * No counterpart in the reference. */
+int hb_ctx_set_wait_limit(hb_ctx *ctx, long long clock_cycles);
+/* Test hook for the path above: while on, bootstrapping launches of this context issue no key
+ * copies, so their first wait for a key chunk runs out (a flag that nothing sets) and the call
+ * returns HB_ERR_TIMEOUT. No counterpart in the reference. */
+int hb_ctx_test_withhold_keys(hb_ctx *ctx, int on);
 
 #ifdef __cplusplus
 }
