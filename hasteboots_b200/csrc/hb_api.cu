@@ -309,7 +309,8 @@ int launch_ext(hb_ctx *ctx, const void *rgsw, uint32_t bits, uint32_t len, const
   constexpr int N = 1 << LOGN;
   auto kern = hb::ext_product_kernel<F, LOGN, T, G, kStages>;
   static_assert(hb::GroupNtt<F, LOGN, T>::LOGV == 4, "external-product kernels use the 16-word tables");
-  const size_t smem = sizeof(W) * (2 * N + kStages * 2 * N + G * 2 * N) + sizeof(uint64_t) * kStages + 16;
+  const size_t smem = sizeof(W) * (2 * N + kStages * 2 * N + G * 2 * N) + sizeof(uint64_t) * kStages +
+                      2 * sizeof(uint32_t) * kStages + 16;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const size_t batches = (count + G - 1) / G;
   const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(batches, (size_t)ctx->sms));

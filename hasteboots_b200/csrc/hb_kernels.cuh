@@ -69,67 +69,12 @@ struct GateJob {
 };
 
 // Ring of S shared-memory stages fed by the TMA unit with consecutive 2N-word chunks of key
-// material; all G groups of the CTA consume chunk c from stage c % S, then the CTA releases it and
-// one thread refills it with chunk c + S.
-template <class W, int N, int S>
-struct ChunkPipe {
-  W *stages;
-  uint64_t *bars;
-  volatile int *abort_flag;
-  int *status;
-  long long budget;
-  unsigned long long next;   // next chunk to consume
-  unsigned long long total;  // chunks this CTA consumes in the whole launch
-  static constexpr uint32_t WORDS = 2 * N;
-  static constexpr uint32_t BYTES = WORDS * sizeof(W);
-
-  template <class Src>
-  __device__ __forceinline__ void prime(const Src &src) {
-    if (threadIdx.x == 0)
-      for (unsigned long long c = 0; c < (unsigned long long)S && c < total; ++c) {
-        mbar_arrive_expect_tx(&bars[c], BYTES);
-        bulk_g2s(stages + c * WORDS, src(c), BYTES, &bars[c]);
-      }
-  }
-  // Wait until the current chunk has landed; returns its stage.
-  __device__ __forceinline__ const W *acquire() {
-    const int st = (int)(next % S);
-    const uint32_t par = (uint32_t)((next / S) & 1);
-    if (!mbar_wait_bounded(&bars[st], par, budget)) {
-      *abort_flag = 1;
-      atomicOr(status, STATUS_TIMEOUT);
-    }
-    return stages + st * WORDS;
-  }
-  // CTA-wide release of the current chunk and refill; false when the launch must stop.
-  template <class Src>
-  __device__ __forceinline__ bool release(const Src &src) {
-    __syncthreads();
-    if (*abort_flag) {
-      drain();
-      return false;
-    }
-    if (threadIdx.x == 0 && next + S < total) {
-      const int st = (int)(next % S);
-      mbar_arrive_expect_tx(&bars[st], BYTES);
-      bulk_g2s(stages + st * WORDS, src(next + S), BYTES, &bars[st]);
-    }
-    ++next;
-    return true;
-  }
-  // On abort: wait (bounded) for the copies this CTA still has in flight before leaving.
-  __device__ __forceinline__ void drain() {
-    if (threadIdx.x != 0) return;
-    for (unsigned long long c = next; c < next + S && c < total; ++c)
-      mbar_wait_bounded(&bars[c % S], (uint32_t)((c / S) & 1), kDrainBudget);
-  }
-};
-
-// The same ring consumed by G independent thread groups without a CTA-wide barrier: each group
-// releases a stage after its own barrier by counting itself in `cnt`; the group whose count
-// completes a multiple of G refills the stage. Groups can therefore drift up to S - 1 chunks apart (one may run
-// its multiply-heavy accumulate while another runs the add-heavy transform). `issued` counts the
-// copies per stage so that an aborting CTA can wait for the ones in flight.
+// material (cp.async.bulk, no multicast), consumed by G independent thread groups without a
+// CTA-wide barrier: each group releases a stage after its own barrier by counting itself in
+// `cnt`; the group whose count completes a multiple of G refills the stage. Groups can therefore
+// drift up to S - 1 chunks apart (one may run its multiply-heavy accumulate while another runs the
+// add-heavy transform). `issued` counts the copies per stage so that an aborting CTA can wait for
+// the ones in flight.
 template <class W, int N, int S, int G>
 struct GroupPipe {
   W *stages;
@@ -302,90 +247,6 @@ __global__ void __launch_bounds__(GPB * T) ntt_batch_kernel(const typename F::W 
 // External product: out_i = RLWE_i x RGSW (lattice/src/rlwe.rs:573-596) for many RLWEs
 // ------------------------------------------------------------------------------------------
 
-template <class F, int LOGN, int T, int G, int S>
-__global__ void __launch_bounds__(G * T, 1)
-    ext_product_kernel(const typename F::W *__restrict__ rlwe_in, typename F::W *__restrict__ rlwe_out,
-                       unsigned long long count, const typename F::W *__restrict__ rgsw,
-                       uint32_t len, uint32_t bits, const typename F::W *__restrict__ tw_g,
-                       const typename F::W *__restrict__ itw_g, int *status, long long budget) {
-  using W = typename F::W;
-  using NT = GroupNtt<F, LOGN, T>;
-  constexpr int N = 1 << LOGN, V = NT::V;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_itw = s_tw + N;
-  W *s_k = s_itw + N;
-  W *s_x = s_k + S * 2 * N;
-  uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_x + G * 2 * N);
-  volatile int *s_abort = reinterpret_cast<volatile int *>(s_bar + S);
-  const int tid = threadIdx.x, g = tid / T, t = tid % T;
-  for (int i = tid; i < N; i += blockDim.x) {
-    s_tw[i] = tw_g[i];
-    s_itw[i] = itw_g[i];
-  }
-  if (tid == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&s_bar[s], 1);
-    mbar_fence_init();
-    *s_abort = 0;
-  }
-  __syncthreads();
-  GroupSync<T> sync{1 + g};
-  W *xbuf = s_x + g * 2 * N;
-  int ping = 0;
-
-  const unsigned long long batches = (count + G - 1) / G;
-  const unsigned long long my_batches =
-      blockIdx.x < batches ? (batches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  const uint32_t cpb = 2 * len;
-  ChunkPipe<W, N, S> pipe{s_k, s_bar, s_abort, status, budget, 0, my_batches * cpb};
-  auto src = [&](unsigned long long c) { return rgsw + (size_t)(c % cpb) * 2 * N; };
-  pipe.prime(src);
-  const uint64_t mask = (bits >= 64) ? ~0ULL : ((1ULL << bits) - 1);
-
-  for (unsigned long long b = blockIdx.x; b < batches; b += gridDim.x) {
-    const unsigned long long item = b * G + g;
-    const bool active = item < count;
-    W acc_a[V], acc_b[V];
-#pragma unroll
-    for (int v = 0; v < V; ++v) acc_a[v] = acc_b[v] = 0;
-    for (int part = 0; part < 2; ++part) {
-      W e[V];
-      if (active) {
-        const W *src_poly = rlwe_in + (item * 2 + part) * N;
-#pragma unroll
-        for (int v = 0; v < V; ++v) e[v] = F::value(src_poly[NT::natural_pos(t, v)]);
-      }
-      for (uint32_t j = 0; j < len; ++j) {
-        W x[V];
-        if (active) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) x[v] = (W)(((uint64_t)e[v] >> (j * bits)) & mask);
-          NT::forward_small(x, xbuf, ping, s_tw, t, sync);
-        }
-        const W *k = pipe.acquire();
-        if (active) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            acc_a[v] = F::mac(acc_a[v], x[v], k[v * T + t]);
-            acc_b[v] = F::mac(acc_b[v], x[v], k[N + v * T + t]);
-          }
-        }
-        if (!pipe.release(src)) return;
-      }
-    }
-    if (active) {
-      NT::inverse(acc_a, xbuf, ping, s_itw, t, sync);
-      NT::inverse(acc_b, xbuf, ping, s_itw, t, sync);
-      W *dst = rlwe_out + item * 2 * N;
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        dst[NT::natural_pos(t, v)] = F::canon(acc_a[v]);
-        dst[N + NT::natural_pos(t, v)] = F::canon(acc_b[v]);
-      }
-    }
-  }
-}
-
 // Digit j of the unsigned LSB-first decomposition (Polynomial::decompose_lsb_bits_inplace,
 // algebra/src/polynomial/univariate/native_polynomial.rs:340-348) of the words e[v * T + t]:
 // (e >> sh) & mask with sh = j * bits uniform, as one funnel shift of the word's halves (or one
@@ -407,6 +268,125 @@ __device__ __forceinline__ void digits(W (&x)[V], const W *e, int t, uint32_t sh
 #pragma unroll
     for (int v = 0; v < V; ++v) x[v] = (e[v * T + t] >> sh) & mask;
   }
+}
+
+// The same on words held in registers.
+template <class W, int V>
+__device__ __forceinline__ void digits_reg(W (&x)[V], const W (&e)[V], uint32_t sh, uint32_t mask) {
+  if constexpr (sizeof(W) == 8) {
+    if (sh < 32) {
+#pragma unroll
+      for (int v = 0; v < V; ++v) x[v] = __funnelshift_r((uint32_t)e[v], (uint32_t)(e[v] >> 32), sh) & mask;
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) x[v] = ((uint32_t)(e[v] >> 32) >> (sh - 32)) & mask;
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < V; ++v) x[v] = (e[v] >> sh) & mask;
+  }
+}
+
+template <class F, int LOGN, int T, int G, int S>
+__global__ void __launch_bounds__(G * T, 1)
+    ext_product_kernel(const typename F::W *__restrict__ rlwe_in, typename F::W *__restrict__ rlwe_out,
+                       unsigned long long count, const typename F::W *__restrict__ rgsw,
+                       uint32_t len, uint32_t bits, const typename F::W *__restrict__ tw_g,
+                       const typename F::W *__restrict__ itw_g, int *status, long long budget) {
+  using W = typename F::W;
+  using NT = GroupNtt<F, LOGN, T>;
+  constexpr int N = 1 << LOGN, V = NT::V;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  W *s_tw = reinterpret_cast<W *>(smem_raw);
+  W *s_itw = s_tw + N;
+  W *s_k = s_itw + N;
+  W *s_x = s_k + S * 2 * N;
+  uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_x + G * 2 * N);
+  uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_bar + S);
+  uint32_t *s_issued = s_cnt + S;
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_issued + S);
+  const int tid = threadIdx.x, g = tid / T, t = tid % T;
+  for (int i = tid; i < N; i += blockDim.x) {
+    s_tw[i] = tw_g[i];
+    s_itw[i] = itw_g[i];
+  }
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&s_bar[s], 1);
+      s_cnt[s] = 0;
+      s_issued[s] = 0;
+    }
+    mbar_fence_init();
+    *s_abort = 0;
+  }
+  __syncthreads();
+  GroupSync<T> sync{1 + g};
+  W *xbuf = s_x + g * 2 * N;
+  int ping = 0;
+
+  const unsigned long long batches = (count + G - 1) / G;
+  const unsigned long long my_batches =
+      blockIdx.x < batches ? (batches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t cpb = 2 * len;
+  GroupPipe<W, N, S, G> pipe{s_k, s_bar, s_cnt, s_issued, s_abort, status, budget, 0, my_batches * cpb};
+  auto src = [&](unsigned long long c) { return rgsw + (size_t)(c % cpb) * 2 * N; };
+  pipe.prime(src);
+  const uint32_t mask = bits >= 32 ? 0xFFFFFFFFu : ((1u << bits) - 1);
+  const W off = F::acc_offset(2 * len);  // every slot sums 2 len products
+
+  for (unsigned long long b = blockIdx.x; b < batches; b += gridDim.x) {
+    const unsigned long long item = b * G + g;
+    const bool active = item < count;
+    typename F::Acc acc_a[V], acc_b[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      F::acc_clear(acc_a[v]);
+      F::acc_clear(acc_b[v]);
+    }
+    for (int part = 0; part < 2; ++part) {
+      W e[V];
+      if (active) {
+        const W *src_poly = rlwe_in + (item * 2 + part) * N;
+#pragma unroll
+        for (int v = 0; v < V; ++v) e[v] = F::value(src_poly[NT::natural_pos(t, v)]);
+      }
+      for (uint32_t j = 0; j < len; ++j) {
+        W x[V];
+        if (active) {
+          digits_reg<W, V>(x, e, j * bits, mask);
+          NT::forward_small(x, xbuf, ping, s_tw, t, sync);
+        }
+        const W *k = pipe.acquire();
+        if (active) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            F::acc_mac(acc_a[v], x[v], k[v * T + t]);
+            F::acc_mac(acc_b[v], x[v], k[N + v * T + t]);
+          }
+        }
+        if (!pipe.release(src, t, sync)) goto aborted;
+      }
+    }
+    if (active) {
+      W fa[V], fb[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        fa[v] = F::acc_value(acc_a[v], off);
+        fb[v] = F::acc_value(acc_b[v], off);
+      }
+      NT::inverse(fa, xbuf, ping, s_itw, t, sync);
+      NT::inverse(fb, xbuf, ping, s_itw, t, sync);
+      W *dst = rlwe_out + item * 2 * N;
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        dst[NT::natural_pos(t, v)] = F::canon(fa[v]);
+        dst[N + NT::natural_pos(t, v)] = F::canon(fb[v]);
+      }
+    }
+  }
+aborted:
+  __syncthreads();
+  if (*s_abort) pipe.drain();
 }
 
 // ------------------------------------------------------------------------------------------
