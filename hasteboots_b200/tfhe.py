@@ -322,9 +322,14 @@ def autotune(ev, sample_gates=0, use_cache=True):
                             ctypes.byref(g), ctypes.byref(rate)), "hb_autotune", ev.ctx.handle)
     if use_cache:
         cache[key] = {"threads_per_gate": t.value, "gates_per_cta": g.value, "gates_per_s": rate.value}
-        tmp = AUTOTUNE_CACHE + ".tmp"
-        json.dump(cache, open(tmp, "w"), indent=1)
-        os.replace(tmp, AUTOTUNE_CACHE)
+        # best effort: processes of one job (one per GPU) may write the same cache at once
+        tmp = f"{AUTOTUNE_CACHE}.{os.getpid()}.tmp"
+        try:
+            with open(tmp, "w") as f:
+                json.dump(cache, f, indent=1)
+            os.replace(tmp, AUTOTUNE_CACHE)
+        except OSError:
+            pass
     return (t.value, g.value), rate.value, False
 
 
