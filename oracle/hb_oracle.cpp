@@ -263,7 +263,7 @@ void schoolbook_negacyclic(const typename F::T *x, const typename F::T *y, typen
 }
 
 // ------------------------------------------------------------------------------------------
-// Seeded PRG and samplers (this build's key convention; the distributions follow
+// Seeded PRG and samplers (the project's key convention; the distributions follow
 // algebra/src/utils/sample.rs:6-51 and algebra/src/random.rs:82-96,156-171).
 // ------------------------------------------------------------------------------------------
 
@@ -308,7 +308,7 @@ inline double unit_double(uint64_t r) { return (double)(r >> 11) * (1.0 / 900719
 
 // FieldDiscreteGaussianSampler::sample (algebra/src/random.rs:156-171): N(0, sigma), reject
 // |x| >= 6 sigma, round half away from zero, negative r -> Q - |r|. The normal deviate comes from
-// the Marsaglia polar method on this build's PRG.
+// the Marsaglia polar method on the project's PRG.
 template <class F>
 typename F::T gaussian(uint64_t seed, uint64_t stream, uint64_t coeff, double sigma) {
   const double max_dev = sigma * 6.0;

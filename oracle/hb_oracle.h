@@ -63,7 +63,7 @@ typedef struct orc_params {
  * (tfhe/src/bfhe/parameters.rs:45-117). Returns 0 or -1 for an unknown id. */
 int orc_params_preset(int preset, orc_params *out);
 
-/* The splitmix-style counter PRG that defines this build's seeded key convention. */
+/* The splitmix-style counter PRG that defines the project's seeded key convention. */
 uint64_t orc_prg(uint64_t seed, uint64_t stream, uint64_t ctr);
 
 /* Key generation from a seed. Output sizes (words): lwe_sk n, ring_sk N,

@@ -3,7 +3,7 @@
     python tests/golden/gen_golden.py
 
 For each parameter set (BABYBEAR / GOLDILOCKS / ZAMA _BINARY_128_BITS) with key seed 0 it records:
-SHA-256 digests of the secret keys, BSK and KSK (this build's seeded key convention); the input
+SHA-256 digests of the secret keys, BSK and KSK (the project's seeded key convention); the input
 ciphertexts of the four NAND truth-table rows (encryption seed 0, sample indices 0..7); the oracle's
 NAND outputs. The BabyBear set also records every other gate, a caller-LUT bootstrap, the modulus
 switch of the first NAND input and the blind-rotation accumulator after 1, 2 and 10 steps.
