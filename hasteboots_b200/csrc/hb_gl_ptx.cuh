@@ -15,6 +15,16 @@ constexpr uint64_t P = 0xFFFFFFFF00000001ULL;
 __device__ __forceinline__ void split(uint64_t x, uint32_t &lo, uint32_t &hi) {
   asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(x));
 }
+// 2^32 - 1 in constant memory: a value the compiler cannot fold, so that 2^32 - 1 - x (~x) can be
+// formed as x (2^32 - 1) + (2^32 - 1) on the multiply pipe instead of the busier logic pipe.
+static __constant__ uint32_t kAllOnes = 0xFFFFFFFFu;
+__device__ __forceinline__ uint32_t not_fma(uint32_t x) {
+  uint32_t r;
+  const uint32_t m = kAllOnes;
+  asm("mad.lo.u32 %0, %1, %2, %2;" : "=r"(r) : "r"(x), "r"(m));
+  return r;
+}
+
 __device__ __forceinline__ uint64_t join(uint32_t lo, uint32_t hi) {
   uint64_t x;
   asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "r"(lo), "r"(hi));
@@ -42,7 +52,7 @@ __device__ __forceinline__ uint64_t mul_lazy(uint64_t a, uint64_t b) {
       : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
       : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
   uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
   uint32_t A0, A1;
   split(A, A0, A1);
   uint32_t r0, r1;
@@ -70,7 +80,7 @@ __device__ __forceinline__ uint64_t mul_lazy(uint64_t a, uint64_t b) {
 // one subtraction of 2^32 - 1 with a borrow fix-up.
 __device__ __forceinline__ uint64_t reduce_canon(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
   uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
   uint32_t A0, A1;
   split(A, A0, A1);
   uint32_t r0, r1;
@@ -95,7 +105,7 @@ __device__ __forceinline__ uint64_t reduce_canon(uint32_t x0, uint32_t x1, uint3
 // reduce_canon with x0 = 0: the low limb of lo + A is A0 and cannot carry.
 __device__ __forceinline__ uint64_t reduce_canon_x0zero(uint32_t x1, uint32_t x2, uint32_t x3) {
   uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
   uint32_t A0, A1;
   split(A, A0, A1);
   uint32_t r0, r1;
@@ -143,7 +153,7 @@ __device__ __forceinline__ void mac_lazy(uint64_t &acc, uint32_t &cnt, uint64_t 
       : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
       : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
   uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)(~x3)));
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
   uint32_t A0, A1, c0, c1;
   split(A, A0, A1);
   split(acc, c0, c1);
