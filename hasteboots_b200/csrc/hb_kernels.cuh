@@ -2,13 +2,15 @@
 //
 //  * prepare_polys_kernel   coefficient-domain key polynomials -> device NTT slot layout, scaled by
 //                           N^-1 (and R for BabyBear) so the inverse transform needs no normalising
-//  * ntt_roundtrip_kernel   batched forward + inverse negacyclic NTT (kernel microbench)
-//  * ntt_fwd/inv_kernel     AbstractNTT::{transform_slice, inverse_transform_slice} on device slices
+//  * relayout_kernel        moves a resident key between the slot layouts of two NTT tiles
+//  * ntt_batch_kernel       batched forward, inverse or round-trip negacyclic NTT on device slices
+//                           (AbstractNTT::{transform_slice, inverse_transform_slice})
 //  * ext_product_kernel     RLWE x RGSW external product for many RLWEs sharing one RGSW
 //  * bootstrap_kernel       persistent batched gate bootstrapping: modulus switch, blind rotation
 //                           with accumulators in shared memory, key switching and sample extraction,
 //                           G gates per CTA sharing every bootstrapping-key chunk, which the TMA unit
 //                           streams into a ring of shared-memory stages
+//  * modmul_probe_kernel    field-multiply throughput (the roofline denominator)
 #pragma once
 
 #include "hb_field.cuh"
