@@ -256,6 +256,7 @@ int prepare_any(hb_ctx *ctx, uint32_t logn, int T, const void *d_in, void *d_out
   if (logn == 10 && T == 64) return launch_prepare<F, 10, 64>(ctx, d_in, d_out, npolys);
   if (logn == 10 && T == 128) return launch_prepare<F, 10, 128>(ctx, d_in, d_out, npolys);
   if (logn == 11 && T == 128) return launch_prepare<F, 11, 128>(ctx, d_in, d_out, npolys);
+  if (logn == 11 && T == 256) return launch_prepare<F, 11, 256>(ctx, d_in, d_out, npolys);
   return fail(ctx, HB_ERR_UNSUPPORTED, "ring dimension 2^%u with %d threads has no compiled kernel", logn, T);
 }
 
@@ -264,18 +265,18 @@ int prepare_field(hb_ctx *ctx, int field, uint32_t logn, int T, const void *d_in
                                       : prepare_any<BabyBear>(ctx, logn, T, d_in, d_out, npolys);
 }
 
-// The standard group size of the NTT and external-product kernels (16 words per thread).
-int std_threads(uint32_t logn) { return logn == 10 ? 64 : 128; }
+// The group size of the NTT and external-product kernels: 8 words per thread, so their passes of
+// three stages take the radix-8 form (GroupNtt::fwd_r8 / inv_r8) for Goldilocks.
+int std_threads(uint32_t logn) { return logn == 10 ? 128 : 256; }
 
 template <class F, int LOGN, int T, int GPB>
 int launch_ntt(hb_ctx *ctx, const void *in, void *out, size_t count, int mode) {
   DevTables *tb;
-  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb);
+  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb, hb::GroupNtt<F, LOGN, T>::LOGV);
   if (rc) return rc;
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   auto kern = hb::ntt_batch_kernel<F, LOGN, T, GPB>;
-  static_assert(hb::GroupNtt<F, LOGN, T>::LOGV == 4, "NTT kernels use the 16-word tables");
   const size_t smem = sizeof(W) * (2 * N + GPB * 2 * N);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
@@ -290,11 +291,11 @@ int launch_ntt(hb_ctx *ctx, const void *in, void *out, size_t count, int mode) {
 
 int ntt_dispatch(hb_ctx *ctx, int field, uint32_t logn, const void *in, void *out, size_t count, int mode) {
   if (field == HB_FIELD_GOLDILOCKS) {
-    if (logn == 10) return launch_ntt<Goldilocks, 10, 64, 4>(ctx, in, out, count, mode);
-    if (logn == 11) return launch_ntt<Goldilocks, 11, 128, 2>(ctx, in, out, count, mode);
+    if (logn == 10) return launch_ntt<Goldilocks, 10, 128, 2>(ctx, in, out, count, mode);
+    if (logn == 11) return launch_ntt<Goldilocks, 11, 256, 1>(ctx, in, out, count, mode);
   } else if (field == HB_FIELD_BABYBEAR) {
-    if (logn == 10) return launch_ntt<BabyBear, 10, 64, 4>(ctx, in, out, count, mode);
-    if (logn == 11) return launch_ntt<BabyBear, 11, 128, 2>(ctx, in, out, count, mode);
+    if (logn == 10) return launch_ntt<BabyBear, 10, 128, 2>(ctx, in, out, count, mode);
+    if (logn == 11) return launch_ntt<BabyBear, 11, 256, 1>(ctx, in, out, count, mode);
   }
   return fail(ctx, HB_ERR_UNSUPPORTED, "no NTT kernel for field %d, log_n %u", field, logn);
 }
@@ -303,12 +304,11 @@ template <class F, int LOGN, int T, int G>
 int launch_ext(hb_ctx *ctx, const void *rgsw, uint32_t bits, uint32_t len, const void *in, void *out,
                size_t count) {
   DevTables *tb;
-  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb);
+  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb, hb::GroupNtt<F, LOGN, T>::LOGV);
   if (rc) return rc;
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   auto kern = hb::ext_product_kernel<F, LOGN, T, G, kStages>;
-  static_assert(hb::GroupNtt<F, LOGN, T>::LOGV == 4, "external-product kernels use the 16-word tables");
   const size_t smem = sizeof(W) * (2 * N + kStages * 2 * N + G * 2 * N) + sizeof(uint64_t) * kStages +
                       2 * sizeof(uint32_t) * kStages + 16;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -859,11 +859,11 @@ int hb_external_product_device(hb_ctx *ctx, int field_id, uint32_t log_n, uint32
   if (count == 0) return HB_OK;
   cudaSetDevice(ctx->device);
   if (field_id == HB_FIELD_GOLDILOCKS) {
-    if (log_n == 10) return launch_ext<Goldilocks, 10, 64, 4>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
-    if (log_n == 11) return launch_ext<Goldilocks, 11, 128, 2>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
+    if (log_n == 10) return launch_ext<Goldilocks, 10, 128, 4>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
+    if (log_n == 11) return launch_ext<Goldilocks, 11, 256, 2>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
   } else if (field_id == HB_FIELD_BABYBEAR) {
-    if (log_n == 10) return launch_ext<BabyBear, 10, 64, 4>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
-    if (log_n == 11) return launch_ext<BabyBear, 11, 128, 2>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
+    if (log_n == 10) return launch_ext<BabyBear, 10, 128, 4>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
+    if (log_n == 11) return launch_ext<BabyBear, 11, 256, 2>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
   }
   return fail(ctx, HB_ERR_UNSUPPORTED, "no external-product kernel for field %d, log_n %u", field_id, log_n);
 }
