@@ -117,7 +117,10 @@ struct GroupPipe {
     if (t == 0) {
       const int st = (int)(next % S);
       __threadfence_block();
-      if ((atomicAdd(&cnt[st], 1u) + 1) % G == 0) {  // counts only grow: no reset to order
+      // Counts only grow (no reset to order against other groups). They stay far below 2^32: a
+      // stage takes G releases per S chunks, about 40 per gate of a launch, and no launch can
+      // hold 10^8 gates' ciphertexts in HBM.
+      if ((atomicAdd(&cnt[st], 1u) + 1) % G == 0) {
         __threadfence_block();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         if (next + S < total) {
