@@ -416,9 +416,18 @@ struct BootParams {
 // Shared memory needed by bootstrap_kernel: twiddles (2N words), S key-chunk stages (2N words
 // each), per gate the accumulator (2N), the exchange buffers (2N) and the decomposition source
 // (N), the modulus-switched input (n + 1 halves) and the stage barriers.
+// Exchange buffers of the bootstrap kernel's transforms: two per gate (one barrier per exchange) or
+// one (a second barrier per exchange). One buffer with the freed 32 KB spent on four key stages
+// measured 0.75 % slower for GOLDILOCKS at G = 4, so two is the default.
+#ifndef HB_BOOT_PINGPONG
+#define HB_BOOT_PINGPONG 1
+#endif
+constexpr bool kBootPingPong = HB_BOOT_PINGPONG != 0;
+constexpr int kBootXbuf = kBootPingPong ? 2 : 1;  // exchange buffers of N words per gate
+
 template <class W, int N, int G, int S>
 __host__ __device__ constexpr size_t boot_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(2 * N + S * 2 * N + G * 5 * N) + sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) +
+  return sizeof(W) * (size_t)(2 * N + S * 2 * N + G * (3 + kBootXbuf) * N) + sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) +
          sizeof(uint64_t) * S + 2 * sizeof(uint32_t) * S + 16;
 }
 
@@ -432,14 +441,14 @@ __host__ __device__ constexpr int boot_stages() {
 template <class F, int LOGN, int T, int G, int S>
 __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
-  using NT = GroupNtt<F, LOGN, T>;
+  using NT = GroupNtt<F, LOGN, T, kBootPingPong>;
   constexpr int N = 1 << LOGN, V = NT::V;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   W *s_tw = reinterpret_cast<W *>(smem_raw);
   W *s_itw = s_tw + N;
   W *s_k = s_itw + N;
   W *s_grp = s_k + S * 2 * N;
-  W *s_e = s_grp + G * 4 * N;
+  W *s_e = s_grp + G * (2 + kBootXbuf) * N;
   const uint32_t msz = (p.n + 8) & ~7u;
   uint16_t *s_ms = reinterpret_cast<uint16_t *>(s_e + G * N);
   uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_ms + G * msz);
@@ -464,7 +473,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   __syncthreads();
 
   GroupSync<T> sync{1 + g};
-  W *acc_a = s_grp + g * 4 * N;
+  W *acc_a = s_grp + g * (2 + kBootXbuf) * N;
   W *acc_b = acc_a + N;
   W *xbuf = acc_b + N;
   W *ebuf = s_e + g * N;  // decomposition source, thread t owns words v * T + t

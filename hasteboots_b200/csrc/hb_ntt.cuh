@@ -33,7 +33,9 @@ struct GroupSync {
   }
 };
 
-template <class F, int LOGN, int T>
+// PP: two exchange buffers used in turn (one barrier per exchange); otherwise one buffer and a
+// second barrier after each exchange's reads.
+template <class F, int LOGN, int T, bool PP = true>
 struct GroupNtt {
   using W = typename F::W;
   static constexpr int N = 1 << LOGN;
@@ -243,8 +245,13 @@ struct GroupNtt {
       fwd_stages<TOP, TOP - 1, SMALL>(x, tw, t);
     if constexpr (LO > 0) {
       constexpr int NEXT = LO - LOGV > 0 ? LO - LOGV : 0;
-      exchange<LO, NEXT>(x, buf + ping * N, t, sync);
-      ping ^= 1;
+      if constexpr (PP) {
+        exchange<LO, NEXT>(x, buf + ping * N, t, sync);
+        ping ^= 1;
+      } else {
+        exchange<LO, NEXT>(x, buf, t, sync);
+        sync();
+      }
       fwd_pass<LO, false>(x, buf, ping, tw, t, sync);
     }
   }
@@ -268,14 +275,19 @@ struct GroupNtt {
       inv_stages<B0, B0>(x, itw, t);
     if constexpr (END < LOGN) {
       constexpr int NLO = END < LOGN - LOGV ? END : LOGN - LOGV;
-      exchange<LO, NLO>(x, buf + ping * N, t, sync);
-      ping ^= 1;
+      if constexpr (PP) {
+        exchange<LO, NLO>(x, buf + ping * N, t, sync);
+        ping ^= 1;
+      } else {
+        exchange<LO, NLO>(x, buf, t, sync);
+        sync();
+      }
       inv_pass<END>(x, buf, ping, itw, t, sync);
     }
   }
 
   // x: natural-order values at natural_pos(t, v) -> slots at slot_pos(t, v).
-  // buf: two exchange buffers of N words (ping-pong), private to the group.
+  // buf: the group's exchange buffers (2 N words with PP, else N).
   __device__ __forceinline__ static void forward(W (&x)[V], W *buf, int &ping, const W *tw, int t,
                                                  const GroupSync<T> &sync) {
     fwd_pass<LOGN, false>(x, buf, ping, tw, t, sync);
