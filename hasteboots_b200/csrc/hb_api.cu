@@ -452,7 +452,10 @@ constexpr int field_of() { return F::FIELD_ID; }
 int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain) {
   if (keys->p.ring_dim != 1024)
     return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
-  const int G = plain ? 1 : keys->gates_per_cta, T = keys->threads_per_gate, fld = keys->p.field_id;
+  uint64_t gates = 0;
+  for (auto &j : jobs) gates += j.count;
+  const int G = plain ? 1 : launch_gates_per_cta(ctx, keys, gates), T = keys->threads_per_gate,
+            fld = keys->p.field_id;
 #define HB_CASE(FLD, TT, GG) \
   if (fld == field_of<FLD>() && T == TT && G == GG) return launch_boot<FLD, 10, TT, GG>(ctx, keys, jobs, plain);
   HB_BOOT_VARIANTS(HB_CASE)
@@ -519,7 +522,7 @@ int launch_table_any(hb_ctx *ctx, hb_keys *keys, int G, const GateJob *djobs, in
                      uint32_t batches, unsigned grid, cudaStream_t stream) {
   const int T = keys->threads_per_gate, fld = keys->p.field_id;
 #define HB_CASE(FLD, TT, GG)                                   \
-  if (fld == field_of<FLD>() && T == TT && G == GG && GG > 1) \
+  if (fld == field_of<FLD>() && T == TT && G == GG)           \
     return launch_table<FLD, 10, TT, GG>(ctx, keys, djobs, njobs, batches, grid, stream);
   HB_BOOT_VARIANTS(HB_CASE)
 #undef HB_CASE
@@ -1211,6 +1214,7 @@ struct hb_batch {
     int njobs = 0;
     uint32_t batches = 0;
     unsigned grid = 0;
+    int gates_per_cta = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
   };
@@ -1271,8 +1275,11 @@ extern "C" int hb_batch_create(hb_ctx *ctx, const hb_job *jobs, size_t njobs, hb
   for (size_t k = 0; k < keysets.size() && !rc; ++k) {
     hb_batch::Group grp;
     grp.keys = keysets[k];
-    const int G = grp.keys->gates_per_cta;
     auto &tab = tables_h[k];
+    uint64_t set_gates = 0;
+    for (auto &t : tab) set_gates += t.count;
+    const int G = launch_gates_per_cta(ctx, grp.keys, set_gates);
+    grp.gates_per_cta = G;
     uint32_t bsum = 0;
     for (auto &t : tab) {
       t.first_batch = bsum;
@@ -1300,7 +1307,7 @@ extern "C" int hb_batch_create(hb_ctx *ctx, const hb_job *jobs, size_t njobs, hb
       if (e != cudaSuccess || rc) break;
       e = cudaStreamWaitEvent(grp.stream, b->fork, 0);
       if (e == cudaSuccess)
-        rc = launch_table_any(ctx, grp.keys, grp.keys->gates_per_cta, (const GateJob *)grp.djobs, grp.njobs,
+        rc = launch_table_any(ctx, grp.keys, grp.gates_per_cta, (const GateJob *)grp.djobs, grp.njobs,
                               grp.batches, grp.grid, grp.stream);
       if (e == cudaSuccess && !rc) e = cudaEventRecord(grp.done, grp.stream);
       if (e == cudaSuccess && !rc) e = cudaStreamWaitEvent(ctx->stream, grp.done, 0);
@@ -1344,10 +1351,24 @@ extern "C" int hb_batch_info(const hb_batch *b, uint64_t *gates, int *launches, 
 
 namespace hbrt {
 
-int launch_set(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, uint32_t batches,
+int launch_set(hb_ctx *ctx, hb_keys *keys, int G, const GateJob *djobs, int njobs, uint32_t batches,
                cudaStream_t stream) {
-  return launch_table_any(ctx, keys, keys->gates_per_cta, djobs, njobs, batches, (unsigned)ctx->sms,
-                          stream);
+  return launch_table_any(ctx, keys, G, djobs, njobs, batches, (unsigned)ctx->sms, stream);
+}
+
+// Gates per CTA for one launch of `gates` gates: the keys' autotuned (throughput) choice, unless that
+// leaves SMs idle; then the smallest compiled variant that still gives every CTA an SM of its own,
+// so that fewer gates share an SM and a small launch finishes sooner.
+int launch_gates_per_cta(const hb_ctx *ctx, const hb_keys *keys, uint64_t gates) {
+  const int tuned = keys->gates_per_cta;
+  const uint64_t sms = (uint64_t)std::max(1, ctx->sms);
+  if (gates >= sms * (uint64_t)tuned) return tuned;
+  std::vector<int> cand = variants(keys->p.field_id, keys->threads_per_gate);
+  cand.push_back(1);
+  std::sort(cand.begin(), cand.end());
+  for (int g : cand)
+    if (g <= tuned && (gates + g - 1) / g <= sms) return g;
+  return tuned;
 }
 
 int gate_job(const hb_params &p, int gate, const void *c0, const void *c1, const void *c2, void *out,

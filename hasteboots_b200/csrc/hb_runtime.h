@@ -66,8 +66,9 @@ int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out, uint32_t l
 int check_status(hb_ctx *ctx);
 long long wait_budget(const hb_ctx *ctx);
 // One persistent bootstrapping launch over a device job table (full grid, the keys' variant).
-int launch_set(hb_ctx *ctx, hb_keys *keys, const hb::GateJob *djobs, int njobs, uint32_t batches,
-               cudaStream_t stream);
+int launch_set(hb_ctx *ctx, hb_keys *keys, int gates_per_cta, const hb::GateJob *djobs, int njobs,
+               uint32_t batches, cudaStream_t stream);
+int launch_gates_per_cta(const hb_ctx *ctx, const hb_keys *keys, uint64_t gates);
 // The job record of `count` single-bootstrap gates (NAND..MAJORITY) of parameter set p.
 int gate_job(const hb_params &p, int gate, const void *c0, const void *c1, const void *c2, void *out,
              uint32_t count, hb::GateJob *job);

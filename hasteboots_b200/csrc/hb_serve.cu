@@ -168,7 +168,9 @@ int launch_wave(hb_server *s, std::vector<Request *> reqs, int slot) {
   std::vector<cudaEvent_t> joins;
   int rc = HB_OK;
   for (size_t k = 0; k < sets.size() && !rc; ++k) {
-    const int G = sets[k]->gates_per_cta;
+    uint64_t set_gates = 0;
+    for (auto &j : tabs[k]) set_gates += j.count;
+    const int G = hbrt::launch_gates_per_cta(ctx, sets[k], set_gates);
     uint32_t batches = 0;
     for (auto &j : tabs[k]) {
       j.first_batch = batches;
@@ -185,7 +187,7 @@ int launch_wave(hb_server *s, std::vector<Request *> reqs, int slot) {
       break;
     }
     w.tables.push_back(dtab);
-    rc = hbrt::launch_set(ctx, sets[k], (const hb::GateJob *)dtab, (int)tabs[k].size(), batches, st);
+    rc = hbrt::launch_set(ctx, sets[k], G, (const hb::GateJob *)dtab, (int)tabs[k].size(), batches, st);
     cudaEvent_t j;
     cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
     cudaEventRecord(j, st);
