@@ -34,12 +34,21 @@ PRESET = 1  # GOLDILOCKS_BINARY_128_BITS
 GATE_NAND = 0
 
 
-def modmuls_per_gate(N, n, length, ks_len):
+def modmuls_per_gate(N, n, length, ks_len, ternary=False):
     """Algorithmic modular multiplications of one bootstrap: n steps of (2l+2) size-N NTTs plus the
-    4lN-term multiply-accumulate, and key switching's (l_ks+2) NTTs plus 2 l_ks N products."""
+    4lN-term multiply-accumulate (a ternary LWE key: two RGSWs, so 8lN terms and 2 more inverse
+    NTTs), and key switching over N/n' chunks of n' = next_pow2(n) words: l_ks NTTs per chunk, 2
+    inverse NTTs and 2 l_ks n' products per chunk, all of size n'."""
     logn = N.bit_length() - 1
     ntt = (N // 2) * logn
-    return n * ((2 * length + 2) * ntt + 4 * length * N) + ((ks_len + 2) * ntt + 2 * ks_len * N)
+    kn = 1 << max(0, (n - 1).bit_length())
+    chunks = N // kn
+    ks_ntt = (kn // 2) * (kn.bit_length() - 1)
+    if ternary:
+        step = (2 * length + 4) * ntt + 8 * length * N
+    else:
+        step = (2 * length + 2) * ntt + 4 * length * N
+    return n * step + (chunks * ks_len + 2) * ks_ntt + 2 * chunks * ks_len * kn
 
 
 def reduce_max(x, world):
@@ -464,7 +473,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--preset", type=int, default=PRESET,
-                    help="0 BABYBEAR, 1 GOLDILOCKS (default, the headline workload), 2 ZAMA")
+                    help="0 BABYBEAR, 1 GOLDILOCKS (default, the headline workload), 2 ZAMA, "
+                         "3 DEFAULT_TERNARY, 4 CUSTOM_TERNARY")
     ap.add_argument("--workload", default="gates", choices=["gates", "mixed", "ntt", "single", "serve"],
                     help="gates: 16384 NAND gates (default, the contract line); mixed: 64 jobs across "
                          "the three sets in one graph; ntt: NTT/external-product microbench; single: "
@@ -590,11 +600,11 @@ def main():
     plain_ok = bool((pd.cpu().numpy().view(params.dtype).reshape(P, width) == out[:P]).all())
 
     # roofline: integer-pipe bound (modular multiplies), HBM shown alongside
-    mm = modmuls_per_gate(raw.ring_dim, raw.lwe_dim, raw.br_len, raw.ks_len)
+    mm = modmuls_per_gate(raw.ring_dim, raw.lwe_dim, raw.br_len, raw.ks_len, bool(raw.lwe_ternary))
     modmul_launch = mm * G
     achieved = modmul_launch / (ms_per_step / 1e3)
     ws = np.dtype(params.dtype).itemsize
-    bsk_bytes = raw.lwe_dim * 2 * raw.br_len * 2 * raw.ring_dim * ws
+    bsk_bytes = raw.lwe_dim * (2 if raw.lwe_ternary else 1) * 2 * raw.br_len * 2 * raw.ring_dim * ws
     ksk_bytes = raw.ks_len * 2 * raw.ring_dim * ws
     io_bytes = G * 3 * width * ws
     alg_bytes = bsk_bytes + ksk_bytes + io_bytes
@@ -604,7 +614,8 @@ def main():
     except (OSError, ValueError):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    traffic = load_traffic("bootstrap_goldilocks_nand_traffic.json")
+    traffic = load_traffic("bootstrap_goldilocks_nand_traffic.json") if args.preset == PRESET else None
+    set_name = params.name.replace("_PARAMETERS", "")
     line = {
         "metric": METRIC,
         "value": value,
@@ -616,14 +627,17 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "u64",
+        "dtype": "u64" if ws == 8 else "u32",
         "data": "synthetic (seed-0 keys, seed-3 uniform input bits)",
         "config": {
-            "workload": f"{G} NAND gate bootstraps, GOLDILOCKS_BINARY_128_BITS (N=1024, n=728, B=2^8, l=8, "
-                        "KS 2^5 x 13), one persistent launch per step",
+            "workload": f"{G} NAND gate bootstraps, {set_name} (N={raw.ring_dim}, n={raw.lwe_dim}, "
+                        f"B=2^{raw.br_bits}, l={raw.br_len}, KS 2^{raw.ks_bits} x {raw.ks_len}), "
+                        "one persistent launch per step",
             "gates_per_gpu": G,
             "parallelism": f"replicas x{world}",
-            "l2": "inputs (191 MB) and BSK (191 MB) exceed L2; no flush",
+            "l2": f"inputs ({2 * G * width * ws / 1e6:.0f} MB) and BSK ({bsk_bytes / 1e6:.0f} MB) "
+                  + ("exceed L2; no flush" if min(2 * G * width * ws, bsk_bytes) > 126e6
+                     else "vs 126 MB L2; no flush"),
             "kernel_variant": {"threads_per_gate": tuned_t, "gates_per_cta": tuned_g},
             "autotune": {"gates_per_s_sample": tuned_rate, "from_cache": tuned_cached},
         },

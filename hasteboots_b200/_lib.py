@@ -17,6 +17,9 @@ ERRORS = {-1: "HB_ERR_INVALID", -2: "HB_ERR_CUDA", -3: "HB_ERR_NOMEM", -4: "HB_E
 
 FIELD_BABYBEAR = 0
 FIELD_GOLDILOCKS = 1
+FIELD_DEFAULT_U32 = 2
+MODULUS = {FIELD_BABYBEAR: 0x78000001, FIELD_GOLDILOCKS: 0xFFFFFFFF00000001,
+           FIELD_DEFAULT_U32: 132120577}
 
 EXPORTS = [
     "hb_params_preset", "hb_params_validate", "hb_params_sizes", "hb_keygen", "hb_encrypt",
@@ -42,6 +45,7 @@ class HbParams(ctypes.Structure):
         ("ks_bits", ctypes.c_uint32),
         ("ks_len", ctypes.c_uint32),
         ("ring_ternary", ctypes.c_uint32),
+        ("lwe_ternary", ctypes.c_uint32),
         ("lwe_noise_std", ctypes.c_double),
         ("ring_noise_std", ctypes.c_double),
         ("ks_noise_std", ctypes.c_double),

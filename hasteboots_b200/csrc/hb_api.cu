@@ -16,6 +16,7 @@
 #include "hb_runtime.h"
 
 using hb::BabyBear;
+using hb::DefaultFieldU32;
 using hb::GateJob;
 using hb::Goldilocks;
 
@@ -193,12 +194,13 @@ int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
 }
 
 int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out, uint32_t logv) {
-  if (logn < 6 || logn > 12 || logv < 1 || logv > 5 || (field_id != 0 && field_id != 1))
+  if (logn < 6 || logn > 12 || logv < 1 || logv > 5 || field_id < 0 || field_id > 2)
     return fail(ctx, HB_ERR_UNSUPPORTED, "no NTT tables for field %d log_n %u", field_id, logn);
   DevTables &t = ctx->tables[field_id][logn][logv];
   if (!t.tw) {
     int rc = field_id == HB_FIELD_GOLDILOCKS ? build_tables<Goldilocks>(ctx, logn, logv, t)
-                                             : build_tables<BabyBear>(ctx, logn, logv, t);
+             : field_id == HB_FIELD_BABYBEAR ? build_tables<BabyBear>(ctx, logn, logv, t)
+                                             : build_tables<DefaultFieldU32>(ctx, logn, logv, t);
     if (rc) return rc;
   }
   *out = &t;
@@ -220,6 +222,24 @@ int check_status(hb_ctx *ctx) {
 
 // ~2 s of SM clocks per bounded wait unless the context sets another limit (hb_ctx_set_wait_limit)
 long long wait_budget(const hb_ctx *ctx) { return ctx && ctx->wait_limit > 0 ? ctx->wait_limit : 4000000000LL; }
+
+uint64_t modulus_of(int field_id) {
+  return field_id == HB_FIELD_GOLDILOCKS ? Goldilocks::P
+         : field_id == HB_FIELD_BABYBEAR ? (uint64_t)BabyBear::P
+                                         : (uint64_t)DefaultFieldU32::P;
+}
+
+// The key switch's dimension n' = next_pow2(n) (fhe_core/src/key_switch/rlwe.rs:40-43).
+uint32_t ks_dim(const hb_params &p) {
+  uint32_t m = 1;
+  while (m < p.lwe_dim) m <<= 1;
+  return m;
+}
+
+// Device words of the key-switching key: every n'-word chunk key polynomial spread to N words.
+size_t ksk_device_words(const hb_params &p) {
+  return (size_t)(p.ring_dim / ks_dim(p)) * p.ks_len * 2 * p.ring_dim;
+}
 
 }  // namespace hbrt
 
@@ -261,8 +281,9 @@ int prepare_any(hb_ctx *ctx, uint32_t logn, int T, const void *d_in, void *d_out
 }
 
 int prepare_field(hb_ctx *ctx, int field, uint32_t logn, int T, const void *d_in, void *d_out, size_t npolys) {
-  return field == HB_FIELD_GOLDILOCKS ? prepare_any<Goldilocks>(ctx, logn, T, d_in, d_out, npolys)
-                                      : prepare_any<BabyBear>(ctx, logn, T, d_in, d_out, npolys);
+  if (field == HB_FIELD_GOLDILOCKS) return prepare_any<Goldilocks>(ctx, logn, T, d_in, d_out, npolys);
+  if (field == HB_FIELD_BABYBEAR) return prepare_any<BabyBear>(ctx, logn, T, d_in, d_out, npolys);
+  return prepare_any<DefaultFieldU32>(ctx, logn, T, d_in, d_out, npolys);
 }
 
 // The group size of the NTT and external-product kernels: 8 words per thread, so their passes of
@@ -296,6 +317,9 @@ int ntt_dispatch(hb_ctx *ctx, int field, uint32_t logn, const void *in, void *ou
   } else if (field == HB_FIELD_BABYBEAR) {
     if (logn == 10) return launch_ntt<BabyBear, 10, 128, 2>(ctx, in, out, count, mode);
     if (logn == 11) return launch_ntt<BabyBear, 11, 256, 1>(ctx, in, out, count, mode);
+  } else if (field == HB_FIELD_DEFAULT_U32) {
+    if (logn == 10) return launch_ntt<DefaultFieldU32, 10, 128, 2>(ctx, in, out, count, mode);
+    if (logn == 11) return launch_ntt<DefaultFieldU32, 11, 256, 1>(ctx, in, out, count, mode);
   }
   return fail(ctx, HB_ERR_UNSUPPORTED, "no NTT kernel for field %d, log_n %u", field, logn);
 }
@@ -328,9 +352,8 @@ struct LutSpec {
   uint64_t lo, hi;
 };
 
-template <class F>
-LutSpec lut_of(int gate, uint32_t N) {
-  const uint64_t q8 = (uint64_t)F::P >> 3, nq8 = (uint64_t)F::P - q8;
+LutSpec lut_of(uint64_t P, int gate, uint32_t N) {
+  const uint64_t q8 = P >> 3, nq8 = P - q8;
   switch (gate) {  // tfhe/src/bfhe/evaluate.rs:267-465
     case HB_GATE_NAND: return {3 * N / 4, q8, nq8};
     case HB_GATE_AND:
@@ -344,16 +367,16 @@ LutSpec lut_of(int gate, uint32_t N) {
   return {N, 0, 0};
 }
 
-template <class F>
-GateJob make_job(int gate, uint32_t N, const void *c0, const void *c1, const void *c2, void *out,
-                 uint32_t count) {
+// P: the field modulus (modulus_of)
+GateJob make_job(uint64_t P, int gate, uint32_t N, const void *c0, const void *c1, const void *c2,
+                 void *out, uint32_t count) {
   GateJob j{};
   j.in0 = c0;
   j.in1 = c1;
   j.in2 = nullptr;
   j.out = out;
   j.lut = nullptr;
-  LutSpec l = lut_of<F>(gate, N);
+  LutSpec l = lut_of(P, gate, N);
   j.lut_mid = l.mid;
   j.lut_lo = l.lo;
   j.lut_hi = l.hi;
@@ -372,7 +395,27 @@ GateJob make_job(int gate, uint32_t N, const void *c0, const void *c1, const voi
   return j;
 }
 
-template <class F, int LOGN, int T, int G>
+// The launch-independent fields of a bootstrap launch's parameters.
+template <class W>
+void boot_params(hb::BootParams<W> &prm, hb_ctx *ctx, const hb_keys *keys, const DevTables *tb) {
+  prm.bsk = (const W *)keys->bsk;
+  prm.ksk = (const W *)keys->ksk;
+  prm.tw = (const W *)tb->tw;
+  prm.itw = (const W *)tb->itw;
+  prm.acc = nullptr;
+  prm.n = keys->p.lwe_dim;
+  prm.len = keys->p.br_len;
+  prm.bits = keys->p.br_bits;
+  prm.ks_len = keys->p.ks_len;
+  prm.ks_bits = keys->p.ks_bits;
+  prm.ks_n = ks_dim(keys->p);
+  prm.ks_chunks = keys->p.ring_dim / prm.ks_n;
+  prm.status = ctx->d_status;
+  prm.budget = wait_budget(ctx);
+  prm.withhold = ctx->withhold_keys;
+}
+
+template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
 int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
@@ -393,26 +436,14 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
                                   cudaMemcpyHostToDevice, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "job table upload");
   hb::BootParams<W> prm{};
-  prm.bsk = (const W *)keys->bsk;
-  prm.ksk = (const W *)keys->ksk;
-  prm.tw = (const W *)tb->tw;
-  prm.itw = (const W *)tb->itw;
-  prm.n = keys->p.lwe_dim;
-  prm.len = keys->p.br_len;
-  prm.bits = keys->p.br_bits;
-  prm.ks_len = keys->p.ks_len;
-  prm.ks_bits = keys->p.ks_bits;
-  prm.status = ctx->d_status;
-  prm.budget = wait_budget(ctx);
-  prm.withhold = ctx->withhold_keys;
+  boot_params(prm, ctx, keys, tb);
   constexpr int S = hb::boot_stages<W, N, G>();
-  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
   const GateJob *djobs = (const GateJob *)ctx->jobs.ptr;
   const unsigned grid = plain ? 1u : std::min<unsigned>(batches, (unsigned)ctx->sms);
-  prm.acc = nullptr;
   const unsigned block = G * T;
   if (!plain) {
     prm.jobs = djobs;
@@ -439,12 +470,27 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
 }
 
 // Compiled variants of the persistent bootstrapping kernel: (field, threads per gate T, gates per
-// CTA G). The key layout fixes T at upload; the autotuner picks G among the variants of that T.
-// G = 1 is the plain one-gate-per-launch form.
-#define HB_BOOT_VARIANTS(X)                                                                    \
-  X(Goldilocks, 64, 1) X(Goldilocks, 64, 3) X(Goldilocks, 64, 4) X(Goldilocks, 128, 1)        \
-  X(Goldilocks, 128, 3) X(Goldilocks, 128, 4) X(BabyBear, 64, 1) X(BabyBear, 64, 4)           \
-  X(BabyBear, 64, 6) X(BabyBear, 64, 8) X(BabyBear, 128, 1) X(BabyBear, 128, 4) X(BabyBear, 128, 6)
+// CTA G, ternary LWE key, key switch in chunks of n' < N words). The key layout fixes T at upload;
+// the autotuner picks G among the variants of that T. G = 1 is the plain one-gate-per-launch form.
+#define HB_BOOT_VARIANTS(X)                                                                          \
+  X(Goldilocks, 64, 1, false, false) X(Goldilocks, 64, 3, false, false)                             \
+  X(Goldilocks, 64, 4, false, false) X(Goldilocks, 128, 1, false, false)                            \
+  X(Goldilocks, 128, 3, false, false) X(Goldilocks, 128, 4, false, false)                           \
+  X(Goldilocks, 128, 1, false, true) X(Goldilocks, 128, 4, false, true)                             \
+  X(BabyBear, 64, 1, false, false) X(BabyBear, 64, 4, false, false) X(BabyBear, 64, 6, false, false) \
+  X(BabyBear, 64, 8, false, false) X(BabyBear, 128, 1, false, false)                                \
+  X(BabyBear, 128, 4, false, false) X(BabyBear, 128, 6, false, false)                               \
+  X(BabyBear, 64, 1, false, true) X(BabyBear, 64, 6, false, true)                                   \
+  X(DefaultFieldU32, 64, 1, false, false) X(DefaultFieldU32, 64, 4, false, false)                   \
+  X(DefaultFieldU32, 64, 6, false, false) X(DefaultFieldU32, 64, 8, false, false)                   \
+  X(DefaultFieldU32, 128, 1, false, false) X(DefaultFieldU32, 128, 4, false, false)                 \
+  X(DefaultFieldU32, 128, 6, false, false) X(DefaultFieldU32, 64, 1, false, true)                   \
+  X(DefaultFieldU32, 64, 4, false, true) X(DefaultFieldU32, 64, 8, false, true)                     \
+  X(DefaultFieldU32, 128, 1, false, true) X(DefaultFieldU32, 128, 4, false, true)                   \
+  X(DefaultFieldU32, 64, 1, true, false) X(DefaultFieldU32, 64, 4, true, false)                     \
+  X(DefaultFieldU32, 128, 1, true, false) X(DefaultFieldU32, 128, 4, true, false)                   \
+  X(DefaultFieldU32, 64, 1, true, true) X(DefaultFieldU32, 64, 4, true, true)                       \
+  X(DefaultFieldU32, 128, 1, true, true) X(DefaultFieldU32, 128, 4, true, true)
 
 template <class F>
 constexpr int field_of() { return F::FIELD_ID; }
@@ -456,18 +502,21 @@ int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain)
   for (auto &j : jobs) gates += j.count;
   const int G = plain ? 1 : launch_gates_per_cta(ctx, keys, gates), T = keys->threads_per_gate,
             fld = keys->p.field_id;
-#define HB_CASE(FLD, TT, GG) \
-  if (fld == field_of<FLD>() && T == TT && G == GG) return launch_boot<FLD, 10, TT, GG>(ctx, keys, jobs, plain);
+  const bool tern = keys->p.lwe_ternary != 0, ksc = ks_dim(keys->p) < keys->p.ring_dim;
+#define HB_CASE(FLD, TT, GG, TN, KC)                                             \
+  if (fld == field_of<FLD>() && T == TT && G == GG && tern == TN && ksc == KC) \
+    return launch_boot<FLD, 10, TT, GG, TN, KC>(ctx, keys, jobs, plain);
   HB_BOOT_VARIANTS(HB_CASE)
 #undef HB_CASE
   return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d threads per gate and %d gates per CTA", T, G);
 }
 
-// Gates-per-CTA variants compiled for a field and group size (the autotuner's candidates).
-std::vector<int> variants(int field_id, int T) {
+// Gates-per-CTA variants compiled for a parameter set and group size (the autotuner's candidates).
+std::vector<int> variants(const hb_params &p, int T) {
   std::vector<int> v;
-#define HB_CASE(FLD, TT, GG) \
-  if (field_id == field_of<FLD>() && T == TT && GG > 1) v.push_back(GG);
+  const bool tern = p.lwe_ternary != 0, ksc = ks_dim(p) < p.ring_dim;
+#define HB_CASE(FLD, TT, GG, TN, KC) \
+  if (p.field_id == field_of<FLD>() && T == TT && GG > 1 && tern == TN && ksc == KC) v.push_back(GG);
   HB_BOOT_VARIANTS(HB_CASE)
 #undef HB_CASE
   return v;
@@ -480,7 +529,7 @@ uint32_t batches_of(const std::vector<GateJob> &jobs, int G) {
 }
 
 // One batched persistent launch over a device job table that is already in place.
-template <class F, int LOGN, int T, int G>
+template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
 int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, uint32_t batches,
                  unsigned grid, cudaStream_t stream) {
   using W = typename F::W;
@@ -489,24 +538,12 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
   int rc = tables(ctx, F::FIELD_ID, LOGN, &tb, hb::GroupNtt<F, LOGN, T>::LOGV);
   if (rc) return rc;
   hb::BootParams<W> prm{};
-  prm.bsk = (const W *)keys->bsk;
-  prm.ksk = (const W *)keys->ksk;
-  prm.tw = (const W *)tb->tw;
-  prm.itw = (const W *)tb->itw;
-  prm.acc = nullptr;
+  boot_params(prm, ctx, keys, tb);
   prm.jobs = djobs;
   prm.njobs = njobs;
   prm.total_batches = batches;
-  prm.n = keys->p.lwe_dim;
-  prm.len = keys->p.br_len;
-  prm.bits = keys->p.br_bits;
-  prm.ks_len = keys->p.ks_len;
-  prm.ks_bits = keys->p.ks_bits;
-  prm.status = ctx->d_status;
-  prm.budget = wait_budget(ctx);
-  prm.withhold = ctx->withhold_keys;
   constexpr int S = hb::boot_stages<W, N, G>();
-  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
@@ -521,9 +558,10 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
 int launch_table_any(hb_ctx *ctx, hb_keys *keys, int G, const GateJob *djobs, int njobs,
                      uint32_t batches, unsigned grid, cudaStream_t stream) {
   const int T = keys->threads_per_gate, fld = keys->p.field_id;
-#define HB_CASE(FLD, TT, GG)                                   \
-  if (fld == field_of<FLD>() && T == TT && G == GG)           \
-    return launch_table<FLD, 10, TT, GG>(ctx, keys, djobs, njobs, batches, grid, stream);
+  const bool tern = keys->p.lwe_ternary != 0, ksc = ks_dim(keys->p) < keys->p.ring_dim;
+#define HB_CASE(FLD, TT, GG, TN, KC)                                             \
+  if (fld == field_of<FLD>() && T == TT && G == GG && tern == TN && ksc == KC) \
+    return launch_table<FLD, 10, TT, GG, TN, KC>(ctx, keys, djobs, njobs, batches, grid, stream);
   HB_BOOT_VARIANTS(HB_CASE)
 #undef HB_CASE
   return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d threads per gate and %d gates per CTA", T, G);
@@ -632,10 +670,25 @@ int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void 
   while ((1u << logn) < p->ring_dim) ++logn;
   hb_keys *k = new hb_keys();
   k->p = *p;
+  // The key switch's n'-word chunk keys (n' = next_pow2(n) < N) are spread to N words, every
+  // (N/n')-th slot, so their products come out of the N-point transforms of the bootstrap kernel
+  // (the ring embedding X -> X^(N/n')).
+  const size_t nkd = ksk_device_words(*p);
+  std::vector<unsigned char> spread;
+  const void *ksk_src = ksk;
+  if (nkd != nk) {
+    const size_t M = ks_dim(*p), stride = p->ring_dim / M, polys = nk / M;
+    spread.assign(nkd * ws, 0);
+    for (size_t q = 0; q < polys; ++q)
+      for (size_t u = 0; u < M; ++u)
+        std::memcpy(spread.data() + (q * p->ring_dim + u * stride) * ws,
+                    (const unsigned char *)ksk + (q * M + u) * ws, ws);
+    ksk_src = spread.data();
+  }
   int rc = dev_alloc(ctx, nb * ws, &k->bsk);
-  if (!rc) rc = dev_alloc(ctx, nk * ws, &k->ksk);
+  if (!rc) rc = dev_alloc(ctx, nkd * ws, &k->ksk);
   void *staging = nullptr;
-  if (!rc) rc = dev_alloc(ctx, std::max(nb, nk) * ws, &staging);
+  if (!rc) rc = dev_alloc(ctx, std::max(nb, nkd) * ws, &staging);
   if (rc) {
     dev_free(ctx, k->bsk);
     dev_free(ctx, k->ksk);
@@ -647,9 +700,9 @@ int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void 
   if (e == cudaSuccess)
     rc = prepare_field(ctx, p->field_id, logn, k->threads_per_gate, staging, k->bsk, nb / p->ring_dim);
   if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(ctx->stream);
-  if (e == cudaSuccess && !rc) e = cudaMemcpyAsync(staging, ksk, nk * ws, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && !rc) e = cudaMemcpyAsync(staging, ksk_src, nkd * ws, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess && !rc)
-    rc = prepare_field(ctx, p->field_id, logn, k->threads_per_gate, staging, k->ksk, nk / p->ring_dim);
+    rc = prepare_field(ctx, p->field_id, logn, k->threads_per_gate, staging, k->ksk, nkd / p->ring_dim);
   if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(ctx->stream);
   dev_free(ctx, staging);
   if (e != cudaSuccess || rc) {
@@ -658,12 +711,11 @@ int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void 
     delete k;
     return e != cudaSuccess ? cuda_fail(ctx, e, "key upload") : rc;
   }
-  k->bytes = (nb + nk) * ws;
+  k->bytes = (nb + nkd) * ws;
   k->gates_per_cta = default_gates_per_cta(p->field_id);
-  if (variants(p->field_id, k->threads_per_gate).size() &&
-      std::find(variants(p->field_id, k->threads_per_gate).begin(), variants(p->field_id, k->threads_per_gate).end(),
-                k->gates_per_cta) == variants(p->field_id, k->threads_per_gate).end())
-    k->gates_per_cta = variants(p->field_id, k->threads_per_gate).back();
+  const std::vector<int> cand = variants(*p, k->threads_per_gate);
+  if (cand.size() && std::find(cand.begin(), cand.end(), k->gates_per_cta) == cand.end())
+    k->gates_per_cta = cand.back();
   *out = k;
   return HB_OK;
 }
@@ -696,21 +748,22 @@ int hb_gate_device(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const v
   const hb_params &p = keys->p;
   const uint32_t N = p.ring_dim;
   const size_t width = p.lwe_dim + 1;
-  const bool gl = p.field_id == HB_FIELD_GOLDILOCKS;
+  const uint64_t P = modulus_of(p.field_id);
   if (gate == HB_GATE_NOT) {
     const size_t words = count * width;
     const unsigned grid = (unsigned)std::min<size_t>((words + 255) / 256, 4096);
-    if (gl)
+    if (p.field_id == HB_FIELD_GOLDILOCKS)
       lwe_not_kernel<Goldilocks><<<grid, 256, 0, ctx->stream>>>((const uint64_t *)c0, (uint64_t *)out, words, (uint32_t)width);
-    else
+    else if (p.field_id == HB_FIELD_BABYBEAR)
       lwe_not_kernel<BabyBear><<<grid, 256, 0, ctx->stream>>>((const uint32_t *)c0, (uint32_t *)out, words, (uint32_t)width);
+    else
+      lwe_not_kernel<DefaultFieldU32><<<grid, 256, 0, ctx->stream>>>((const uint32_t *)c0, (uint32_t *)out, words, (uint32_t)width);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? HB_OK : cuda_fail(ctx, e, "not launch");
   }
   std::vector<GateJob> jobs;
   if (gate != HB_GATE_MUX) {
-    jobs.push_back(gl ? make_job<Goldilocks>(gate, N, c0, c1, c2, out, (uint32_t)count)
-                      : make_job<BabyBear>(gate, N, c0, c1, c2, out, (uint32_t)count));
+    jobs.push_back(make_job(P, gate, N, c0, c1, c2, out, (uint32_t)count));
     return run_jobs(ctx, keys, jobs, false);
   }
   // MUX (evaluate.rs:245-262): t0 = and(c0, c1), t1 = and(not c0, c2), out = bootstrap(t0 + t1, or)
@@ -718,18 +771,16 @@ int hb_gate_device(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const v
   int rc = scratch(ctx, ctx->mux_tmp, 2 * bytes);
   if (rc) return rc;
   char *t0 = (char *)ctx->mux_tmp.ptr, *t1 = t0 + bytes;
-  GateJob a = gl ? make_job<Goldilocks>(HB_GATE_AND, N, c0, c1, nullptr, t0, (uint32_t)count)
-                 : make_job<BabyBear>(HB_GATE_AND, N, c0, c1, nullptr, t0, (uint32_t)count);
+  GateJob a = make_job(P, HB_GATE_AND, N, c0, c1, nullptr, t0, (uint32_t)count);
   GateJob b = a;
   b.in1 = c2;
   b.out = t1;
   b.s0 = -1;  // not(c0) = -c0 + Q/4 on the body
-  b.add_b = gl ? (Goldilocks::P >> 2) : (BabyBear::P >> 2);
+  b.add_b = P >> 2;
   jobs = {a, b};
   rc = run_jobs(ctx, keys, jobs, false);
   if (rc) return rc;
-  jobs = {gl ? make_job<Goldilocks>(HB_GATE_MUX, N, t0, t1, nullptr, out, (uint32_t)count)
-             : make_job<BabyBear>(HB_GATE_MUX, N, t0, t1, nullptr, out, (uint32_t)count)};
+  jobs = {make_job(P, HB_GATE_MUX, N, t0, t1, nullptr, out, (uint32_t)count)};
   return run_jobs(ctx, keys, jobs, false);
 }
 
@@ -746,8 +797,7 @@ int hb_gate_device_plain(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, c
     const char *a = (const char *)c0 + i * width * ws;
     const char *b = (const char *)c1 + i * width * ws;
     char *o = (char *)out + i * width * ws;
-    jobs.push_back(p.field_id == HB_FIELD_GOLDILOCKS ? make_job<Goldilocks>(gate, p.ring_dim, a, b, nullptr, o, 1)
-                                                      : make_job<BabyBear>(gate, p.ring_dim, a, b, nullptr, o, 1));
+    jobs.push_back(make_job(modulus_of(p.field_id), gate, p.ring_dim, a, b, nullptr, o, 1));
   }
   return run_jobs(ctx, keys, jobs, true);
 }
@@ -826,6 +876,7 @@ int hb_rgsw_upload(hb_ctx *ctx, int field_id, uint32_t log_n, uint32_t bits, uin
   if (!ctx || !rgsw || !d_rgsw || bits == 0 || bits > 16 || len == 0 || (uint64_t)(len - 1) * bits >= 64)
     return HB_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  if (field_id < 0 || field_id > 2) return fail(ctx, HB_ERR_INVALID, "unknown field %d", field_id);
   const size_t N = (size_t)1 << log_n, ws = field_id == HB_FIELD_GOLDILOCKS ? 8 : 4;
   const size_t words = 2 * (size_t)len * 2 * N;
   void *dst = nullptr, *staging = nullptr;
@@ -867,12 +918,15 @@ int hb_external_product_device(hb_ctx *ctx, int field_id, uint32_t log_n, uint32
   } else if (field_id == HB_FIELD_BABYBEAR) {
     if (log_n == 10) return launch_ext<BabyBear, 10, 128, 4>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
     if (log_n == 11) return launch_ext<BabyBear, 11, 256, 2>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
+  } else if (field_id == HB_FIELD_DEFAULT_U32) {
+    if (log_n == 10) return launch_ext<DefaultFieldU32, 10, 128, 4>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
+    if (log_n == 11) return launch_ext<DefaultFieldU32, 11, 256, 2>(ctx, d_rgsw, bits, len, rlwe_in, rlwe_out, count);
   }
   return fail(ctx, HB_ERR_UNSUPPORTED, "no external-product kernel for field %d, log_n %u", field_id, log_n);
 }
 
 int hb_probe_modmul(hb_ctx *ctx, int field_id, double *modmul_per_s) {
-  if (!ctx || !modmul_per_s || (field_id != 0 && field_id != 1)) return HB_ERR_INVALID;
+  if (!ctx || !modmul_per_s || field_id < 0 || field_id > 2) return HB_ERR_INVALID;
   cudaSetDevice(ctx->device);
   const unsigned blocks = (unsigned)ctx->sms * 8, threads = 256;
   const uint32_t iters = field_id == HB_FIELD_GOLDILOCKS ? 4096 : 16384;
@@ -887,8 +941,10 @@ int hb_probe_modmul(hb_ctx *ctx, int field_id, double *modmul_per_s) {
     cudaEventRecord(e0, ctx->stream);
     if (field_id == HB_FIELD_GOLDILOCKS)
       hb::modmul_probe_kernel<Goldilocks><<<blocks, threads, 0, ctx->stream>>>((uint64_t *)buf, iters, 12345 + rep);
-    else
+    else if (field_id == HB_FIELD_BABYBEAR)
       hb::modmul_probe_kernel<BabyBear><<<blocks, threads, 0, ctx->stream>>>((uint32_t *)buf, iters, 12345 + rep);
+    else
+      hb::modmul_probe_kernel<DefaultFieldU32><<<blocks, threads, 0, ctx->stream>>>((uint32_t *)buf, iters, 12345 + rep);
     cudaEventRecord(e1, ctx->stream);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -955,29 +1011,20 @@ int noalloc_address(hb_ctx *ctx, unsigned char **out) {
   return HB_OK;
 }
 
-template <class F, int LOGN, int T, int G>
+template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
 int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJob *djobs, int njobs,
                    uint32_t batches, int *dstatus) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   hb::BootParams<W> prm{};
-  prm.bsk = (const W *)keys->bsk;
-  prm.ksk = (const W *)keys->ksk;
-  prm.tw = (const W *)tb->tw;
-  prm.itw = (const W *)tb->itw;
-  prm.acc = nullptr;
+  boot_params(prm, ctx, keys, tb);
   prm.jobs = djobs;
   prm.njobs = njobs;
   prm.total_batches = batches;
-  prm.n = keys->p.lwe_dim;
-  prm.len = keys->p.br_len;
-  prm.bits = keys->p.br_bits;
-  prm.ks_len = keys->p.ks_len;
-  prm.ks_bits = keys->p.ks_bits;
   prm.status = dstatus;
-  prm.budget = wait_budget(ctx);
+  prm.withhold = 0;
   constexpr int S = hb::boot_stages<W, N, G>();
-  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S>;
+  auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
@@ -990,9 +1037,10 @@ int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJo
 int noalloc_layer(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJob *djobs, int njobs,
                   uint32_t batches, int *dstatus) {
   const int G = keys->gates_per_cta, T = keys->threads_per_gate, fld = keys->p.field_id;
-#define HB_CASE(FLD, TT, GG)                                   \
-  if (fld == field_of<FLD>() && T == TT && G == GG && GG > 1) \
-    return launch_noalloc<FLD, 10, TT, GG>(ctx, keys, tb, djobs, njobs, batches, dstatus);
+  const bool tern = keys->p.lwe_ternary != 0, ksc = ks_dim(keys->p) < keys->p.ring_dim;
+#define HB_CASE(FLD, TT, GG, TN, KC)                                                       \
+  if (fld == field_of<FLD>() && T == TT && G == GG && GG > 1 && tern == TN && ksc == KC) \
+    return launch_noalloc<FLD, 10, TT, GG, TN, KC>(ctx, keys, tb, djobs, njobs, batches, dstatus);
   HB_BOOT_VARIANTS(HB_CASE)
 #undef HB_CASE
   return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d gates per CTA", G);
@@ -1007,8 +1055,8 @@ extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void
   if (count == 0) return HB_OK;
   const hb_params &p = keys->p;
   if (p.ring_dim != 1024) return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
-  const bool gl = p.field_id == HB_FIELD_GOLDILOCKS;
-  const size_t width = (size_t)p.lwe_dim + 1, ws = gl ? 8 : 4;
+  const uint64_t P = modulus_of(p.field_id);
+  const size_t width = (size_t)p.lwe_dim + 1, ws = word_size(p);
   const size_t max_gates = (kNoAllocBytes - kNoAllocData) / (2 * width * ws);
   if (count > max_gates)
     return fail(ctx, HB_ERR_INVALID,
@@ -1031,15 +1079,13 @@ extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void
   // then out = bootstrap(t0 + t1, or) in a second.
   const int G = keys->gates_per_cta;
   GateJob jobs[3];
-  jobs[0] = gl ? make_job<Goldilocks>(HB_GATE_AND, p.ring_dim, c0, c1, nullptr, t0, (uint32_t)count)
-               : make_job<BabyBear>(HB_GATE_AND, p.ring_dim, c0, c1, nullptr, t0, (uint32_t)count);
+  jobs[0] = make_job(P, HB_GATE_AND, p.ring_dim, c0, c1, nullptr, t0, (uint32_t)count);
   jobs[1] = jobs[0];
   jobs[1].in1 = c2;
   jobs[1].out = t1;
   jobs[1].s0 = -1;  // not(c0) = -c0 + Q/4 on the body
-  jobs[1].add_b = gl ? (Goldilocks::P >> 2) : (BabyBear::P >> 2);
-  jobs[2] = gl ? make_job<Goldilocks>(HB_GATE_MUX, p.ring_dim, t0, t1, nullptr, out, (uint32_t)count)
-               : make_job<BabyBear>(HB_GATE_MUX, p.ring_dim, t0, t1, nullptr, out, (uint32_t)count);
+  jobs[1].add_b = P >> 2;
+  jobs[2] = make_job(P, HB_GATE_MUX, p.ring_dim, t0, t1, nullptr, out, (uint32_t)count);
   const uint32_t per_job = (uint32_t)((count + G - 1) / G);
   jobs[0].first_batch = 0;
   jobs[1].first_batch = per_job;
@@ -1071,8 +1117,9 @@ namespace {
 int relayout_keys(hb_ctx *ctx, hb_keys *keys, int T) {
   if (keys->threads_per_gate == T) return HB_OK;
   const size_t ws = word_size(keys->p);
-  size_t nb = 0, nk = 0;
-  hb_params_sizes(&keys->p, nullptr, nullptr, &nb, &nk, nullptr);
+  size_t nb = 0;
+  hb_params_sizes(&keys->p, nullptr, nullptr, &nb, nullptr, nullptr);
+  const size_t nk = ksk_device_words(keys->p);
   uint32_t logn = 0;
   while ((1u << logn) < keys->p.ring_dim) ++logn;
   DevTables *tb;
@@ -1108,8 +1155,8 @@ int relayout_keys(hb_ctx *ctx, hb_keys *keys, int T) {
   return HB_OK;
 }
 
-bool compiled(int field_id, int T, int G) {
-  for (int g : variants(field_id, T))
+bool compiled(const hb_params &p, int T, int G) {
+  for (int g : variants(p, T))
     if (g == G) return true;
   return false;
 }
@@ -1118,7 +1165,7 @@ bool compiled(int field_id, int T, int G) {
 
 extern "C" int hb_keys_set_config(hb_ctx *ctx, hb_keys *keys, int threads_per_gate, int gates_per_cta) {
   if (!ctx || !keys) return HB_ERR_INVALID;
-  if (!compiled(keys->p.field_id, threads_per_gate, gates_per_cta))
+  if (!compiled(keys->p, threads_per_gate, gates_per_cta))
     return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d threads per gate and %d gates per CTA",
                 threads_per_gate, gates_per_cta);
   cudaSetDevice(ctx->device);
@@ -1163,14 +1210,11 @@ extern "C" int hb_autotune(hb_ctx *ctx, hb_keys *keys, uint32_t sample_gates, in
   int best_g = keys->gates_per_cta, best_t = keys->threads_per_gate;
   double best_rate = 0;
   for (int T : {64, 128})
-  for (int G : variants(keys->p.field_id, T)) {
+  for (int G : variants(keys->p, T)) {
     if (!rc) rc = relayout_keys(ctx, keys, T);
     if (rc) break;
-    std::vector<GateJob> jobs{keys->p.field_id == HB_FIELD_GOLDILOCKS
-                                  ? make_job<Goldilocks>(HB_GATE_NAND, 1024, buf, buf, nullptr,
-                                                         (char *)buf + bytes, sample_gates)
-                                  : make_job<BabyBear>(HB_GATE_NAND, 1024, buf, buf, nullptr,
-                                                       (char *)buf + bytes, sample_gates)};
+    std::vector<GateJob> jobs{make_job(modulus_of(keys->p.field_id), HB_GATE_NAND, 1024, buf, buf,
+                                       nullptr, (char *)buf + bytes, sample_gates)};
     jobs[0].first_batch = 0;
     const uint32_t batches = batches_of(jobs, G);
     cudaMemcpyAsync(tab, jobs.data(), sizeof(GateJob), cudaMemcpyHostToDevice, ctx->stream);
@@ -1261,9 +1305,8 @@ extern "C" int hb_batch_create(hb_ctx *ctx, const hb_job *jobs, size_t njobs, hb
       keysets.push_back(j.keys);
       tables_h.emplace_back();
     }
-    const bool gl = j.keys->p.field_id == HB_FIELD_GOLDILOCKS;
-    tables_h[k].push_back(gl ? make_job<Goldilocks>(j.gate, 1024, j.c0, j.c1, j.c2, j.out, j.count)
-                             : make_job<BabyBear>(j.gate, 1024, j.c0, j.c1, j.c2, j.out, j.count));
+    tables_h[k].push_back(make_job(modulus_of(j.keys->p.field_id), j.gate, 1024, j.c0, j.c1, j.c2, j.out,
+                                   j.count));
     gates += j.count;
   }
   hb_batch *b = new hb_batch();
@@ -1363,7 +1406,7 @@ int launch_gates_per_cta(const hb_ctx *ctx, const hb_keys *keys, uint64_t gates)
   const int tuned = keys->gates_per_cta;
   const uint64_t sms = (uint64_t)std::max(1, ctx->sms);
   if (gates >= sms * (uint64_t)tuned) return tuned;
-  std::vector<int> cand = variants(keys->p.field_id, keys->threads_per_gate);
+  std::vector<int> cand = variants(keys->p, keys->threads_per_gate);
   cand.push_back(1);
   std::sort(cand.begin(), cand.end());
   for (int g : cand)
@@ -1374,8 +1417,7 @@ int launch_gates_per_cta(const hb_ctx *ctx, const hb_keys *keys, uint64_t gates)
 int gate_job(const hb_params &p, int gate, const void *c0, const void *c1, const void *c2, void *out,
              uint32_t count, GateJob *job) {
   if (!single_bootstrap_gate(gate) || p.ring_dim != 1024) return HB_ERR_INVALID;
-  *job = p.field_id == HB_FIELD_GOLDILOCKS ? make_job<Goldilocks>(gate, 1024, c0, c1, c2, out, count)
-                                           : make_job<BabyBear>(gate, 1024, c0, c1, c2, out, count);
+  *job = make_job(modulus_of(p.field_id), gate, 1024, c0, c1, c2, out, count);
   return HB_OK;
 }
 

@@ -5,11 +5,12 @@
 //   rand(seed, stream, ctr) = mix(mix(seed + g) ^ mix(stream ^ c) + ctr * g)
 // (mix = splitmix64 finaliser), so key generation parallelises over polynomials and is identical on
 // every host. Streams: (tag, i, part, j, which) packed into 64 bits. Distributions follow the
-// reference: binary LWE key (algebra/src/utils/sample.rs:6-27), ternary ring key {0,0,1,-1}[r&3]
-// (sample.rs:30-51), uniform field elements, and the discrete Gaussian of
-// FieldDiscreteGaussianSampler (algebra/src/random.rs:156-171: N(0, sigma), reject |x| >= 6 sigma,
-// round half away from zero, negative r -> Q - |r|) with normal deviates from the Marsaglia polar
-// method and a logarithm built from IEEE-exact operations.
+// reference: binary or ternary {0,0,1,-1}[r&3] LWE and ring keys (algebra/src/utils/sample.rs:6-51),
+// uniform field elements, and the discrete Gaussian of FieldDiscreteGaussianSampler
+// (algebra/src/random.rs:156-171: N(0, sigma), reject |x| >= 6 sigma, round half away from zero,
+// negative r -> Q - |r|) with normal deviates from the Marsaglia polar method and a logarithm built
+// from IEEE-exact operations; error polynomials with sigma exactly 3.2 come from the centered
+// binomial sampler instead (algebra/src/random.rs:91-92, algebra/src/utils/sample.rs:54-75).
 
 #include <algorithm>
 #include <atomic>
@@ -106,6 +107,42 @@ inline typename F::W sample_uniform(u64 seed, u64 stream, u64 k) {
   return (typename F::W)(rnd(seed, stream, k) % (u64)F::P);
 }
 
+// sample_cbd_field_vec (algebra/src/utils/sample.rs:54-75) on the low six bytes of one PRG word:
+// popcounts a (bytes 0, 1 and 5 bits of byte 2) and b (bytes 3, 4 and 5 bits of byte 5). For a < b
+// the reference's `modulus - (a - b)` wraps its u32 subtraction (release builds), which leaves
+// Field::new of the wrapped word in the field's width: b - a for 32-bit fields,
+// P - (2^32 - (b - a)) for Goldilocks.
+template <class F>
+typename F::W sample_cbd(u64 seed, u64 stream, u64 k) {
+  using W = typename F::W;
+  const u64 r = rnd(seed, stream, k);
+  auto pc = [](u64 x) { return (uint32_t)__builtin_popcountll(x); };
+  const uint32_t a = pc(r & 0xFF) + pc((r >> 8) & 0xFF) + pc((r >> 16) & 0x1F);
+  const uint32_t b = pc((r >> 24) & 0xFF) + pc((r >> 32) & 0xFF) + pc((r >> 40) & 0x1F);
+  const uint32_t d = a - b;
+  if (a >= b) return (W)d;
+  const W v = (W)((W)F::P - (W)d);
+  return (W)((u64)v % (u64)F::P);
+}
+
+// One coefficient of an error polynomial (Polynomial::random_with_gaussian,
+// algebra/src/polynomial/univariate/native_polynomial.rs:232-246).
+template <class F>
+typename F::W error_coeff(u64 seed, u64 stream, u64 k, double sigma) {
+  return sigma == 3.2 ? sample_cbd<F>(seed, stream, k) : sample_gauss<F>(seed, stream, k, sigma);
+}
+
+// Calls fn(F{}) with the field type of a field id (Goldilocks, BabyBear or DefaultFieldU32).
+template <class Fn>
+void with_field(int field_id, Fn fn) {
+  if (field_id == HB_FIELD_GOLDILOCKS)
+    fn(hb::Goldilocks{});
+  else if (field_id == HB_FIELD_BABYBEAR)
+    fn(hb::BabyBear{});
+  else
+    fn(hb::DefaultFieldU32{});
+}
+
 // ---- host negacyclic multiplication for key generation (radix-2, twisted cyclic NTT) ----
 template <class F>
 struct HostRing {
@@ -184,19 +221,30 @@ struct HostRing {
   }
 };
 
+u64 modulus_of(int field_id) {
+  return field_id == HB_FIELD_GOLDILOCKS ? hb::Goldilocks::P
+         : field_id == HB_FIELD_BABYBEAR ? (u64)hb::BabyBear::P
+                                         : (u64)hb::DefaultFieldU32::P;
+}
+
 bool check_params(const hb_params *p) {
   if (!p) return false;
-  if (p->field_id != HB_FIELD_BABYBEAR && p->field_id != HB_FIELD_GOLDILOCKS) return false;
+  if (p->field_id != HB_FIELD_BABYBEAR && p->field_id != HB_FIELD_GOLDILOCKS &&
+      p->field_id != HB_FIELD_DEFAULT_U32)
+    return false;
   const uint32_t N = p->ring_dim;
   if (N < 4 || N > 4096 || (N & (N - 1))) return false;
+  // The RLWE key switch pads the LWE key to next_pow2(n) <= N words
+  // (fhe_core/src/key_switch/rlwe.rs:40-43).
   if (p->lwe_dim == 0 || p->lwe_dim > N) return false;
-  uint32_t np2 = 1;
-  while (np2 < p->lwe_dim) np2 <<= 1;
-  if (np2 != N) return false;  // the RLWE key switch of the reference sets (next_pow2(n) == N)
+  // A ternary LWE key takes TernaryBlindRotationKey, whose NTT-domain monomial the reference marks
+  // incompatible with BabyBear and Goldilocks (fhe_core/src/blind_rotation/rlwe/ternary.rs:80).
+  if (p->lwe_ternary > 1 || (p->lwe_ternary && p->field_id != HB_FIELD_DEFAULT_U32)) return false;
+  if (p->ring_ternary > 1) return false;
   // Parameters::new: 2N | Q - 1 (fhe_core/src/parameter.rs:131-138)
-  const u64 q = p->field_id == HB_FIELD_GOLDILOCKS ? hb::Goldilocks::P : hb::BabyBear::P;
+  const u64 q = modulus_of(p->field_id);
   if ((q - 1) % (2ull * N) != 0) return false;
-  const uint32_t qbits = p->field_id == HB_FIELD_GOLDILOCKS ? 64 : 31;
+  const uint32_t qbits = p->field_id == HB_FIELD_GOLDILOCKS ? 64 : p->field_id == HB_FIELD_BABYBEAR ? 31 : 27;
   if (p->br_bits == 0 || p->br_bits > 16 || p->ks_bits == 0 || p->ks_bits > 16) return false;
   if (p->br_len != (qbits + p->br_bits - 1) / p->br_bits) return false;
   if (p->ks_len != (qbits + p->ks_bits - 1) / p->ks_bits) return false;
@@ -210,16 +258,14 @@ void keygen_impl(const hb_params *p, u64 seed, typename F::W *lwe_sk, typename F
   using W = typename F::W;
   using H = HostField<F>;
   const uint32_t N = p->ring_dim, n = p->lwe_dim, L = p->br_len;
-  for (uint32_t i = 0; i < n; ++i) lwe_sk[i] = (W)(rnd(seed, stream_of(kTagLweSk, 0, 0, 0, 0), i) & 1);
-  static const int kTern[4] = {0, 0, 1, -1};
+  const W tern[4] = {0, 0, 1, (W)(F::P - 1)};
+  for (uint32_t i = 0; i < n; ++i) {
+    const u64 r = rnd(seed, stream_of(kTagLweSk, 0, 0, 0, 0), i);
+    lwe_sk[i] = p->lwe_ternary ? tern[r & 3] : (W)(r & 1);
+  }
   for (uint32_t k = 0; k < N; ++k) {
     const u64 r = rnd(seed, stream_of(kTagRingSk, 0, 0, 0, 0), k);
-    if (p->ring_ternary) {
-      const int v = kTern[r & 3];
-      ring_sk[k] = v < 0 ? (W)(F::P - 1) : (W)v;
-    } else {
-      ring_sk[k] = (W)(r & 1);
-    }
+    ring_sk[k] = p->ring_ternary ? tern[r & 3] : (W)(r & 1);
   }
   if (!bsk) return;
   uint32_t logn = 0;
@@ -228,27 +274,33 @@ void keygen_impl(const hb_params *p, u64 seed, typename F::W *lwe_sk, typename F
   std::vector<W> z_eval(ring_sk, ring_sk + N);
   ring.to_eval(z_eval.data());
 
-  // One RLWE zero sample: a uniform, b = a*key + e.
-  auto zero_sample = [&](const W *key_eval, u64 sa, u64 se, double sigma, W *a, W *b) {
-    for (uint32_t k = 0; k < N; ++k) a[k] = sample_uniform<F>(seed, sa, k);
-    ring.mul(a, key_eval, b);
-    for (uint32_t k = 0; k < N; ++k) b[k] = H::add(b[k], sample_gauss<F>(seed, se, k, sigma));
+  // One RLWE zero sample in the ring of rg: a uniform, b = a*key + e.
+  auto zero_sample = [&](const HostRing<F> &rg, const W *key_eval, u64 sa, u64 se, double sigma, W *a,
+                         W *b) {
+    for (uint32_t k = 0; k < rg.n; ++k) a[k] = sample_uniform<F>(seed, sa, k);
+    rg.mul(a, key_eval, b);
+    for (uint32_t k = 0; k < rg.n; ++k) b[k] = H::add(b[k], error_coeff<F>(seed, se, k, sigma));
   };
 
-  // BSK: per LWE key bit an NTTRGSW zero sample (s_i = 0) or one sample (s_i = 1)
-  // (lattice/src/rgsw.rs:343-395): c_neg_s_m rows (a + B^j, b) / c_m rows (a, b + B^j).
-  const size_t rows_total = (size_t)n * 2 * L;
+  // BSK: per LWE key coefficient an NTTRGSW zero sample (s_i = 0) or one sample (s_i = 1)
+  // (lattice/src/rgsw.rs:343-395): c_neg_s_m rows (a + B^j, b) / c_m rows (a, b + B^j). A ternary
+  // key holds the pair (RGSW(s_i == 1), RGSW(s_i == -1)) per coefficient
+  // (fhe_core/src/blind_rotation/rlwe/ternary.rs:123-183); pair 1 draws from streams part + 2.
+  const uint32_t pairs = p->lwe_ternary ? 2 : 1;
+  const size_t rows_total = (size_t)n * pairs * 2 * L;
   std::atomic<size_t> next{0};
   auto worker = [&] {
     for (size_t q; (q = next.fetch_add(1)) < rows_total;) {
-      const uint32_t i = (uint32_t)(q / (2 * L));
+      const uint32_t i = (uint32_t)(q / (pairs * 2 * L));
+      const uint32_t pair = (uint32_t)((q / (2 * L)) % pairs);
       const uint32_t part = (uint32_t)((q / L) % 2);
       const uint32_t j = (uint32_t)(q % L);
       W *a = bsk + q * 2 * N;
       W *b = a + N;
-      zero_sample(z_eval.data(), stream_of(kTagBsk, i, part, j, 0), stream_of(kTagBsk, i, part, j, 1),
-                  p->ring_noise_std, a, b);
-      if (lwe_sk[i]) {
+      zero_sample(ring, z_eval.data(), stream_of(kTagBsk, i, part + 2 * pair, j, 0),
+                  stream_of(kTagBsk, i, part + 2 * pair, j, 1), p->ring_noise_std, a, b);
+      const bool one = pairs == 1 ? lwe_sk[i] != 0 : lwe_sk[i] == (pair == 0 ? (W)1 : (W)(F::P - 1));
+      if (one) {
         const W bj = (W)((u64)1 << (j * p->br_bits));
         if (part == 0)
           a[0] = H::add(a[0], bj);
@@ -262,20 +314,29 @@ void keygen_impl(const hb_params *p, u64 seed, typename F::W *lwe_sk, typename F
   for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
   for (auto &th : pool) th.join();
 
-  // KSK rows j: zero samples under the extended LWE key, plus z * B_ks^j on b
-  // (fhe_core/src/key_switch/rlwe.rs:57-78).
-  std::vector<W> s_eval(N, 0);
+  // KSK (fhe_core/src/key_switch/rlwe.rs:37-112): the LWE key padded to n' = next_pow2(n) words;
+  // per n'-word chunk z_c of the ring key (z itself when n' == N) rows j = zero samples of
+  // dimension n' plus z_c * B_ks^j on b. Layout [c][j][ab][n'].
+  uint32_t M = 1, logm = 0;
+  while (M < n) {
+    M <<= 1;
+    ++logm;
+  }
+  HostRing<F> kring(logm);
+  std::vector<W> s_eval(M, 0);
   for (uint32_t i = 0; i < n; ++i) s_eval[i] = lwe_sk[i];
-  ring.to_eval(s_eval.data());
-  std::vector<W> zpow(ring_sk, ring_sk + N);
+  kring.to_eval(s_eval.data());
   const W bks = (W)(1u << p->ks_bits);
-  for (uint32_t j = 0; j < p->ks_len; ++j) {
-    W *a = ksk + (size_t)j * 2 * N;
-    W *b = a + N;
-    zero_sample(s_eval.data(), stream_of(kTagKsk, 0, 0, j, 0), stream_of(kTagKsk, 0, 0, j, 1),
-                p->ks_noise_std, a, b);
-    for (uint32_t k = 0; k < N; ++k) b[k] = H::add(b[k], zpow[k]);
-    for (uint32_t k = 0; k < N; ++k) zpow[k] = H::mul(zpow[k], bks);
+  for (uint32_t c = 0; c < N / M; ++c) {
+    std::vector<W> zpow(ring_sk + (size_t)c * M, ring_sk + (size_t)(c + 1) * M);
+    for (uint32_t j = 0; j < p->ks_len; ++j) {
+      W *a = ksk + ((size_t)c * p->ks_len + j) * 2 * M;
+      W *b = a + M;
+      zero_sample(kring, s_eval.data(), stream_of(kTagKsk, c, 0, j, 0), stream_of(kTagKsk, c, 0, j, 1),
+                  p->ks_noise_std, a, b);
+      for (uint32_t k = 0; k < M; ++k) b[k] = H::add(b[k], zpow[k]);
+      for (uint32_t k = 0; k < M; ++k) zpow[k] = H::mul(zpow[k], bks);
+    }
   }
 }
 
@@ -341,6 +402,21 @@ int hb_params_preset(int preset, hb_params *out) {
   out->lwe_dim = 728;
   out->ring_ternary = 1;
   out->ks_bits = 5;
+  if (preset == HB_PRESET_DEFAULT_TERNARY_128_BITS || preset == HB_PRESET_CUSTOM_TERNARY_128_BITS) {
+    // tfhe/src/bfhe/parameters.rs:7-42: both sets configure binary LWE and ring keys.
+    const bool dflt = preset == HB_PRESET_DEFAULT_TERNARY_128_BITS;
+    out->field_id = HB_FIELD_DEFAULT_U32;
+    out->lwe_dim = dflt ? 1024 : 512;
+    out->ring_ternary = 0;
+    out->br_bits = dflt ? 3 : 7;
+    out->br_len = dflt ? 9 : 4;
+    out->ks_bits = dflt ? 1 : 7;
+    out->ks_len = dflt ? 27 : 4;
+    out->lwe_noise_std = 3.20;
+    out->ring_noise_std = 3.20 * 2.0;
+    out->ks_noise_std = 3.2 * 2.0;
+    return HB_OK;
+  }
   if (preset == HB_PRESET_BABYBEAR_BINARY_128_BITS) {
     out->field_id = HB_FIELD_BABYBEAR;
     out->br_bits = 8;
@@ -373,7 +449,7 @@ int hb_params_sizes(const hb_params *p, size_t *lwe_sk, size_t *ring_sk, size_t 
   const size_t N = p->ring_dim, n = p->lwe_dim;
   if (lwe_sk) *lwe_sk = n;
   if (ring_sk) *ring_sk = N;
-  if (bsk) *bsk = n * 2 * p->br_len * 2 * N;
+  if (bsk) *bsk = n * (p->lwe_ternary ? 2 : 1) * 2 * p->br_len * 2 * N;
   if (ksk) *ksk = (size_t)p->ks_len * 2 * N;
   if (lwe) *lwe = n + 1;
   return HB_OK;
@@ -384,36 +460,33 @@ int hb_keygen(const hb_params *p, uint64_t seed, void *lwe_sk, void *ring_sk, vo
   // bsk and ksk may both be NULL: only the secret keys are produced (KeyGen::generate_secret_key).
   if (!check_params(p) || !lwe_sk || !ring_sk || (!bsk != !ksk)) return HB_ERR_INVALID;
   if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-  if (p->field_id == HB_FIELD_GOLDILOCKS)
-    keygen_impl<hb::Goldilocks>(p, seed, (uint64_t *)lwe_sk, (uint64_t *)ring_sk, (uint64_t *)bsk,
-                                (uint64_t *)ksk, threads);
-  else
-    keygen_impl<hb::BabyBear>(p, seed, (uint32_t *)lwe_sk, (uint32_t *)ring_sk, (uint32_t *)bsk,
-                              (uint32_t *)ksk, threads);
+  with_field(p->field_id, [&](auto f) {
+    using F = decltype(f);
+    using W = typename F::W;
+    keygen_impl<F>(p, seed, (W *)lwe_sk, (W *)ring_sk, (W *)bsk, (W *)ksk, threads);
+  });
   return HB_OK;
 }
 
 int hb_encrypt(const hb_params *p, const void *lwe_sk, uint64_t seed, uint64_t index0,
                const uint8_t *bits, size_t count, void *lwe_out) {
   if (!check_params(p) || !lwe_sk || (count && (!bits || !lwe_out))) return HB_ERR_INVALID;
-  if (p->field_id == HB_FIELD_GOLDILOCKS)
-    encrypt_impl<hb::Goldilocks>(p, (const uint64_t *)lwe_sk, seed, index0, bits, count,
-                                 (uint64_t *)lwe_out);
-  else
-    encrypt_impl<hb::BabyBear>(p, (const uint32_t *)lwe_sk, seed, index0, bits, count,
-                               (uint32_t *)lwe_out);
+  with_field(p->field_id, [&](auto f) {
+    using F = decltype(f);
+    using W = typename F::W;
+    encrypt_impl<F>(p, (const W *)lwe_sk, seed, index0, bits, count, (W *)lwe_out);
+  });
   return HB_OK;
 }
 
 int hb_decrypt(const hb_params *p, const void *lwe_sk, const void *lwe, size_t count,
                uint8_t *bits_out, uint64_t *noise_out) {
   if (!check_params(p) || !lwe_sk || (count && !lwe)) return HB_ERR_INVALID;
-  if (p->field_id == HB_FIELD_GOLDILOCKS)
-    decrypt_impl<hb::Goldilocks>(p, (const uint64_t *)lwe_sk, (const uint64_t *)lwe, count, bits_out,
-                                 noise_out);
-  else
-    decrypt_impl<hb::BabyBear>(p, (const uint32_t *)lwe_sk, (const uint32_t *)lwe, count, bits_out,
-                               noise_out);
+  with_field(p->field_id, [&](auto f) {
+    using F = decltype(f);
+    using W = typename F::W;
+    decrypt_impl<F>(p, (const W *)lwe_sk, (const W *)lwe, count, bits_out, noise_out);
+  });
   return HB_OK;
 }
 

@@ -1,4 +1,4 @@
-// hb_field.cuh -- Goldilocks and BabyBear arithmetic for sm_100a on the integer pipe.
+// hb_field.cuh -- Goldilocks, BabyBear and DefaultFieldU32 arithmetic for sm_100a on the integer pipe.
 //
 // Goldilocks Q = 2^64 - 2^32 + 1 (algebra/src/modulus/goldilocks/mod.rs:9-11): 64x64->128 products
 // folded with 2^64 = 2^32 - 1 and 2^96 = -1 (mod Q); values may sit anywhere in [0, 2^64) and are
@@ -7,8 +7,9 @@
 // (algebra/src/modulus/goldilocks/ops.rs:26-73) because a non-canonical accumulator word is
 // negated by `P - x` there, and bit-exact outputs must follow that.
 //
-// BabyBear Q = 2^31 - 2^27 + 1 (algebra/src/modulus/baby_bear/mod.rs:11): data words are canonical
-// residues; constants that multiply data (twiddles, keys) are stored premultiplied by R = 2^32 so a
+// BabyBear Q = 2^31 - 2^27 + 1 (algebra/src/modulus/baby_bear/mod.rs:11) and DefaultFieldU32
+// Q = 2^27 - 2^21 + 1 (fhe_core/src/parameter.rs:286-290): data words are canonical residues;
+// constants that multiply data (twiddles, keys) are stored premultiplied by R = 2^32 so a
 // Montgomery product returns a canonical residue of the plain product.
 #pragma once
 
@@ -180,12 +181,14 @@ struct Goldilocks {
   static constexpr bool RADIX8 = true;
 };
 
-struct BabyBear {
+// 32-bit prime fields P < 2^31 with canonical data words and Montgomery-form constants.
+template <uint32_t PP, uint32_t PINV, int BB, int ID>
+struct Mont32 {
   using W = uint32_t;
-  static constexpr W P = 0x78000001U;
-  static constexpr W PINV_NEG = 0x77FFFFFFU;  // -P^-1 mod 2^32
-  static constexpr int BITS = 31;
-  static constexpr int FIELD_ID = 0;
+  static constexpr W P = PP;
+  static constexpr W PINV_NEG = PINV;  // -P^-1 mod 2^32
+  static constexpr int BITS = BB;      // bits(Q): the decomposition covers this many bits
+  static constexpr int FIELD_ID = ID;
 
   HB_HD static W canon(W x) { return x >= P ? x - P : x; }
   // Montgomery product a*b*2^-32 mod P for a*b < P*2^32; canonical result.
@@ -230,6 +233,11 @@ struct BabyBear {
   static constexpr uint64_t SMALL_FIRST_GEN = 0;  // no special first stage
   static constexpr bool RADIX8 = false;
 };
+
+// BabyBear Q = 2^31 - 2^27 + 1 (algebra/src/modulus/baby_bear/mod.rs:11-15).
+using BabyBear = Mont32<0x78000001U, 0x77FFFFFFU, 31, 0>;
+// DefaultFieldU32 Q = 132120577 = 2^27 - 2^21 + 1 (fhe_core/src/parameter.rs:286-290), bits(Q) = 27.
+using DefaultFieldU32 = Mont32<0x07E00001U, 0x07DFFFFFU, 27, 2>;
 
 // Host-side exact helpers used to build tables.
 template <class F>

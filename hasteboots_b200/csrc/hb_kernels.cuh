@@ -400,14 +400,15 @@ aborted:
 
 template <class W>
 struct BootParams {
-  const W *bsk;  // [n][2][len][2][N] slot layout, scaled (one 2N-word chunk per (i, part, j))
-  const W *ksk;  // [ks_len][2][N] slot layout, scaled
+  const W *bsk;  // [n][pairs][2][len][2][N] slot layout, scaled (one 2N-word chunk per row)
+  const W *ksk;  // [ks_chunks][ks_len][2][N] slot layout, scaled (chunk keys spread to N words)
   const W *tw, *itw;
   W *acc;  // unused by this kernel (accumulators live in shared memory)
   const GateJob *jobs;
   int njobs;
   uint32_t total_batches;
   uint32_t n, len, bits, ks_len, ks_bits;
+  uint32_t ks_n, ks_chunks;  // key-switch dimension n' = next_pow2(n) and its N / n' chunks
   int *status;
   long long budget;
   int withhold;  // test hook: issue no key-chunk copy, so the first wait runs out (bounded)
@@ -438,7 +439,11 @@ __host__ __device__ constexpr int boot_stages() {
   return boot_smem_bytes<W, N, G, 3>(1016) <= 232448 ? 3 : 2;
 }
 
-template <class F, int LOGN, int T, int G, int S>
+// TERN: ternary LWE key (TernaryBlindRotationKey, fhe_core/src/blind_rotation/rlwe/ternary.rs:26-119)
+// with two RGSWs per key coefficient, for fields whose words stay canonical.
+// KSC: key switch in ks_chunks chunks of n' = next_pow2(n) < N words; without it the key switch is
+// the single chunk n' = N of the reference presets, with no chunk bookkeeping in the kernel.
+template <class F, int LOGN, int T, int G, int S, bool TERN = false, bool KSC = false>
 __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T, kBootPingPong>;
@@ -481,15 +486,26 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   int ping = 0;
 
   const uint32_t n = p.n;
-  const uint32_t br_chunks = n * 2 * p.len;
-  const uint32_t cpb = br_chunks + p.ks_len;
+  constexpr uint32_t PAIRS = TERN ? 2 : 1;
+  const uint32_t br_chunks = n * PAIRS * 2 * p.len;
+  const uint32_t ks_chunks = KSC ? p.ks_chunks : 1;
+  const uint32_t cpb = br_chunks + ks_chunks * p.ks_len;
   const uint32_t my_batches =
       blockIdx.x < p.total_batches ? (p.total_batches - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   GroupPipe<W, N, S, G> pipe{s_k, s_bar, s_cnt, s_issued, s_abort, p.status, p.budget, 0,
                              p.withhold ? 0ull : (unsigned long long)my_batches * cpb};
+  // Chunks in consumption order: per step (i, part, j) and, for a ternary key, both RGSWs' rows
+  // of that digit in turn (stored [i][pair][part][j]); then the key switch's [c][j] rows.
   auto src = [&](unsigned long long c) -> const W * {
     const uint32_t q = (uint32_t)(c % cpb);
-    return q < br_chunks ? p.bsk + (size_t)q * 2 * N : p.ksk + (size_t)(q - br_chunks) * 2 * N;
+    if (q >= br_chunks) return p.ksk + (size_t)(q - br_chunks) * 2 * N;
+    if constexpr (TERN) {
+      const uint32_t L = p.len, i = q / (4 * L), r = q % (4 * L);
+      const uint32_t part = r / (2 * L), j = (r >> 1) % L, pair = r & 1;
+      return p.bsk + ((size_t)((i * 2 + pair) * 2 + part) * L + j) * 2 * N;
+    } else {
+      return p.bsk + (size_t)q * 2 * N;
+    }
   };
   pipe.prime(src);
 
@@ -497,7 +513,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   // Offsets that remove the per-product bookkeeping of the lazy accumulators (F::acc_value): a
   // blind-rotation step sums 2 len products per slot, the key switch ks_len.
   const W off_br = F::acc_offset(2 * p.len);
-  const W off_ks = F::acc_offset(p.ks_len);
+  const W off_ks = F::acc_offset(ks_chunks * p.ks_len);
 
   for (uint32_t batch = blockIdx.x; batch < p.total_batches; batch += gridDim.x) {
     int jx = 0;
@@ -545,18 +561,23 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
     sync();
 
     // ---- blind rotation (binary.rs:66-103), then key switching (key_switch/rlwe.rs:115-137) ----
-    // One loop of 2n + 1 phases shares a single forward-NTT and a single inverse-NTT call site:
-    // phase 2i + part decomposes E.a (part 0) or E.b (part 1) of step i, phase 2n decomposes -acc.a
-    // for the key switch.
+    // One loop of 2n + ks_chunks phases shares a single forward-NTT and a single inverse-NTT call
+    // site: phase 2i + part decomposes E.a (part 0) or E.b (part 1) of step i, phase 2n + c
+    // decomposes the key switch's chunk c of -acc.a.
     typename F::Acc acc_x[V], acc_y[V];
+    typename F::Acc acc_x1[TERN ? V : 1], acc_y1[TERN ? V : 1];  // ternary: RGSW(s_i == -1) products
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       F::acc_clear(acc_x[v]);
       F::acc_clear(acc_y[v]);
+      if constexpr (TERN) {
+        F::acc_clear(acc_x1[v]);
+        F::acc_clear(acc_y1[v]);
+      }
     }
-    const uint32_t phases = 2 * n + 1;
+    const uint32_t phases = 2 * n + ks_chunks;
     for (uint32_t ph = 0; ph < phases; ++ph) {
-      const bool ks = ph == 2 * n;
+      const bool ks = KSC ? ph >= 2 * n : ph == 2 * n;
       const uint32_t part = ph & 1;
       if (active) {
         if (!ks) {
@@ -578,10 +599,31 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             }
             ebuf[v * T + t] = F::value(F::sub(rot, y[k]));
           }
-        } else {
+        } else if (!KSC) {
           // sub_assign_gadget_rlwe_mul_polynomial_inplace_fast: p = -acc.a (lattice/src/rlwe.rs:1147-1166)
 #pragma unroll
           for (int v = 0; v < V; ++v) ebuf[v * T + t] = F::value(F::neg_ref(acc_a[NT::natural_pos(t, v)]));
+        } else {
+          // n' < N (fhe_core/src/key_switch/rlwe.rs:123-131): a[0] = -a[0], a[1..] reversed, then on
+          // chunk c the same again, so chunk word u is -a[N - c n'] (u = 0; a[0] negated twice for
+          // c = 0) or a[N - (c + 1) n' + u]; the chunk is then negated (p = -chunk) and placed at
+          // every ks_stride-th slot, the ring embedding X -> X^ks_stride of the n'-word product.
+          const uint32_t c = ph - 2 * n, kn = p.ks_n, ks_stride = N / kn;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const int k = NT::natural_pos(t, v);
+            W d = 0;
+            if ((uint32_t)k % ks_stride == 0) {
+              const uint32_t u = (uint32_t)k / ks_stride;
+              W w;
+              if (u != 0)
+                w = acc_a[N - (c + 1) * kn + u];
+              else
+                w = c == 0 ? F::neg_ref(F::neg_ref(acc_a[0])) : F::neg_ref(acc_a[N - c * kn]);
+              d = F::value(F::neg_ref(w));
+            }
+            ebuf[v * T + t] = d;
+          }
         }
       }
       const uint32_t L = ks ? p.ks_len : p.len;
@@ -603,8 +645,69 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
           }
         }
         if (!pipe.release(src, t, sync)) goto aborted;
+        if constexpr (TERN) {
+          if (!ks) {  // the same digit against RGSW(s_i == -1)
+            const W *k1 = pipe.acquire();
+            if (active) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                F::acc_mac(acc_x1[v], x[v], k1[v * T + t]);
+                F::acc_mac(acc_y1[v], x[v], k1[N + v * T + t]);
+              }
+            }
+            if (!pipe.release(src, t, sync)) goto aborted;
+          }
+        }
       }
-      if (part == 0 && !ks) continue;
+      if (KSC ? (ks ? ph + 1 < phases : part == 0) : (part == 0 && !ks)) continue;
+      if constexpr (TERN) {
+        if (!ks) {
+          // Ternary step (ternary.rs:78-114): the evaluation key RGSW_0 + RGSW_1 * (-X^-a) is
+          // linear in the RGSWs, so ACC += INTT(acc_0) + (-X^(2N - a)) * INTT(acc_1) per
+          // polynomial. h even: INTT of the pair-1 sum into ebuf; h odd: ACC += INTT(pair-0 sum)
+          // minus ebuf rotated by d = 2N - a (negacyclic). The chain acc_x1, acc_x, acc_y1, acc_y
+          // shifts one place per h.
+          const int d = (int)(2 * N) - (int)ms[ph >> 1];
+#pragma unroll 1
+          for (int h = 0; h < 4; ++h) {
+            if (active) {
+              W f[V];
+#pragma unroll
+              for (int v = 0; v < V; ++v) f[v] = F::acc_value(acc_x1[v], off_br);
+              NT::inverse(f, xbuf, ping, s_itw, t, sync);
+              if ((h & 1) == 0) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) ebuf[NT::natural_pos(t, v)] = F::canon(f[v]);
+              } else {
+                W *y = h == 1 ? acc_a : acc_b;
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                  const int k = NT::natural_pos(t, v);
+                  const int s = k - d;
+                  W rot;
+                  if (s >= 0) {
+                    rot = ebuf[s];
+                  } else if (s >= -N) {
+                    rot = F::neg_ref(ebuf[s + N]);
+                  } else {
+                    rot = ebuf[s + 2 * N];
+                  }
+                  y[k] = F::add(y[k], F::sub(F::canon(f[v]), rot));
+                }
+              }
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                acc_x1[v] = acc_x[v];
+                acc_x[v] = acc_y1[v];
+                acc_y1[v] = acc_y[v];
+                F::acc_clear(acc_y[v]);
+              }
+            }
+            sync();  // ebuf written (h even) or read (h odd) by the whole group
+          }
+          continue;
+        }
+      }
       // Inverse transforms of both accumulators through one call site: h = 0 handles acc_x (the
       // a polynomial), then acc_y moves into acc_x for h = 1 (the b polynomial).
       const W off = ks ? off_ks : off_br;
@@ -627,16 +730,21 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             }
           } else {
             // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402): a' = [A0, -A_{N-1}, ...],
-            // b' = b0 + B0
+            // b' = b0 + B0; with KSC the n'-word result sits at every (N/n')-th slot and
+            // a' = [A0, -A_{n'-1}, ..., -A_{n'-n+1}]
+            const int kn = KSC ? (int)p.ks_n : N, ks_stride = N / kn;
 #pragma unroll
             for (int v = 0; v < V; ++v) {
               const int k = NT::natural_pos(t, v);
               const W val = F::canon(f[v]);
               if (h == 0) {
-                if (k == 0)
-                  out[0] = val;
-                else if (k >= N - (int)n + 1)
-                  out[N - k] = F::neg_ref(val);
+                if (!KSC || k % ks_stride == 0) {
+                  const int u = KSC ? k / ks_stride : k;
+                  if (u == 0)
+                    out[0] = val;
+                  else if (u >= kn - (int)n + 1)
+                    out[kn - u] = F::neg_ref(val);
+                }
               } else if (k == 0) {
                 out[n] = F::canon(F::add(val, b0));
               }

@@ -39,7 +39,7 @@ struct hb_ctx {
   size_t in_use = 0;
   std::vector<std::pair<void *, size_t>> sizes;
   std::string err;
-  hbrt::DevTables tables[2][13][6];  // [field][log2 N][log2 words per thread]
+  hbrt::DevTables tables[3][13][6];  // [field][log2 N][log2 words per thread]
   hbrt::Scratch jobs, io, mux_tmp, acc;
   std::atomic<unsigned long long> launches{0};  // bootstrap kernel launches issued by this context
   long long wait_limit = 0;                     // SM clock cycles per bounded wait; 0 = default

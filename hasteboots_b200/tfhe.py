@@ -3,7 +3,8 @@
 Names follow the reference (tfhe/src/lib.rs:1-13): parameter statics, KeyGen, SecretKeyPack,
 Encryptor, Decryptor, Evaluator with nand/and/or/nor/xor/xnor/majority/not/mux/bootstrap
 (tfhe/src/bfhe/evaluate.rs:65-262). Ciphertexts are numpy arrays (host) or torch CUDA tensors
-(device), shape [count, n + 1], dtype uint64 (Goldilocks) / uint32 (BabyBear), canonical values.
+(device), shape [count, n + 1], dtype uint64 (Goldilocks) / uint32 (BabyBear, DefaultFieldU32),
+canonical values.
 Host arrays go through hb_gate (copies in and out included); device tensors through hb_gate_device
 on the context stream.
 """
@@ -29,7 +30,7 @@ def _ptr(a):
 
 
 class Parameters:
-    """fhe_core::Parameters for the binary-LWE-key RLWE bootstrapping sets."""
+    """fhe_core::Parameters for RLWE bootstrapping with the RLWE key switch."""
 
     def __init__(self, raw: HbParams, name=""):
         check(lib().hb_params_validate(ctypes.byref(raw)), "Parameters::new")
@@ -41,8 +42,16 @@ class Parameters:
         raw = HbParams()
         check(lib().hb_params_preset(pid, ctypes.byref(raw)), "hb_params_preset")
         names = {0: "BABYBEAR_BINARY_128_BITS_PARAMETERS",
-                 1: "GOLDILOCKS_BINARY_128_BITS_PARAMETERS", 2: "ZAMA_BINARY_128_BITS_PARAMETERS"}
+                 1: "GOLDILOCKS_BINARY_128_BITS_PARAMETERS", 2: "ZAMA_BINARY_128_BITS_PARAMETERS",
+                 3: "DEFAULT_TERNARY_128_BITS_PARAMETERS", 4: "CUSTOM_TERNARY_128_BITS_PARAMETERS"}
         return cls(raw, names[pid])
+
+    def with_ternary_lwe_key(self):
+        """The same set with a ternary LWE secret key (LWESecretKeyType::Ternary,
+        fhe_core/src/secret_key.rs:12-18); DefaultFieldU32 sets only."""
+        raw = HbParams.from_buffer_copy(self.raw)
+        raw.lwe_ternary = 1
+        return Parameters(raw, self.name + "+TERNARY_LWE_KEY")
 
     @property
     def field_id(self):
@@ -54,7 +63,7 @@ class Parameters:
 
     @property
     def modulus(self):
-        return 0xFFFFFFFF00000001 if self.raw.field_id == _lib.FIELD_GOLDILOCKS else 0x78000001
+        return _lib.MODULUS[self.raw.field_id]
 
     def lwe_dimension(self):
         return self.raw.lwe_dim
@@ -72,6 +81,14 @@ class Parameters:
 
 def BABYBEAR_BINARY_128_BITS_PARAMETERS():
     return Parameters.preset(0)
+
+
+def DEFAULT_TERNARY_128_BITS_PARAMETERS():
+    return Parameters.preset(3)
+
+
+def CUSTOM_TERNARY_128_BITS_PARAMETERS():
+    return Parameters.preset(4)
 
 
 def GOLDILOCKS_BINARY_128_BITS_PARAMETERS():

@@ -13,12 +13,17 @@
  *    non-zero statuses to panics where the reference panics (tfhe/src/bfhe/evaluate.rs:56) and to
  *    Err where it returns Result (Parameters::new, fhe_core/src/parameter.rs:111).
  *  - Field words are canonical little-endian values: uint64_t for Goldilocks
- *    (Q = 2^64 - 2^32 + 1), uint32_t for BabyBear (Q = 2^31 - 2^27 + 1).
+ *    (Q = 2^64 - 2^32 + 1), uint32_t for BabyBear (Q = 2^31 - 2^27 + 1) and DefaultFieldU32
+ *    (Q = 132120577 = 2^27 - 2^21 + 1, fhe_core/src/parameter.rs:286-290).
  *  - An LWE ciphertext is n+1 words: a[0..n) then b. Batches are contiguous arrays of them.
  *  - Key material in host buffers is coefficient domain: BSK layout
- *    [i < n][part: 0 = c_neg_s_m, 1 = c_m][j < br_len][0 = a, 1 = b][N], KSK layout
- *    [j < ks_len][0 = a, 1 = b][N] (NTTRGSW lattice/src/rgsw.rs:212-218, NTTGadgetRLWE
- *    lattice/src/gadget/rlwe.rs:235-240, KeySwitchingRLWEKey fhe_core/src/key_switch/rlwe.rs:23-28).
+ *    [i < n][pair][part: 0 = c_neg_s_m, 1 = c_m][j < br_len][0 = a, 1 = b][N] with one pair for a
+ *    binary LWE key and two -- RGSW(s_i == 1), RGSW(s_i == -1) -- for a ternary one; KSK layout
+ *    [c < N/n'][j < ks_len][0 = a, 1 = b][n'] with n' = next_pow2(n) (NTTRGSW
+ *    lattice/src/rgsw.rs:212-218, TernaryBlindRotationKey
+ *    fhe_core/src/blind_rotation/rlwe/ternary.rs:13-16, NTTGadgetRLWE
+ *    lattice/src/gadget/rlwe.rs:235-240, KeySwitchingRLWEKey fhe_core/src/key_switch/rlwe.rs:23-28,
+ *    one gadget RLWE per n'-word chunk of the ring key, :79-108).
  *  - Functions named *_device take device pointers and enqueue on the context's stream without
  *    synchronising; all other functions take host pointers and return when results are in place.
  *  - A context is used by one host thread at a time.
@@ -43,11 +48,15 @@ extern "C" {
 
 #define HB_FIELD_BABYBEAR 0
 #define HB_FIELD_GOLDILOCKS 1
+#define HB_FIELD_DEFAULT_U32 2 /* DefaultFieldU32, Q = 132120577 */
 
-/* Parameter-set ids (tfhe/src/bfhe/parameters.rs:45-117). */
+/* Parameter-set ids (tfhe/src/bfhe/parameters.rs:7-117). The two *_TERNARY_* sets configure
+ * binary LWE and ring keys over DefaultFieldU32; n = 1024 and n = 512 (two key-switching chunks). */
 #define HB_PRESET_BABYBEAR_BINARY_128_BITS 0
 #define HB_PRESET_GOLDILOCKS_BINARY_128_BITS 1
 #define HB_PRESET_ZAMA_BINARY_128_BITS 2
+#define HB_PRESET_DEFAULT_TERNARY_128_BITS 3
+#define HB_PRESET_CUSTOM_TERNARY_128_BITS 4
 
 /* Gate ids (Evaluator::{nand, and, or, nor, xor, xnor, majority, not, mux},
  * tfhe/src/bfhe/evaluate.rs:98-262). */
@@ -64,16 +73,18 @@ extern "C" {
 typedef struct hb_ctx hb_ctx;
 typedef struct hb_keys hb_keys;
 
-/* fhe_core::ConstParameters (fhe_core/src/parameter.rs:81-107), binary LWE key branch. */
+/* fhe_core::ConstParameters (fhe_core/src/parameter.rs:81-107) with the RLWE key switch. */
 typedef struct hb_params {
   int32_t field_id;      /* HB_FIELD_* */
   uint32_t ring_dim;     /* N (1024 is compiled) */
-  uint32_t lwe_dim;      /* n, with next_pow2(n) == N */
+  uint32_t lwe_dim;      /* n <= N; the key switch works in dimension n' = next_pow2(n) */
   uint32_t br_bits;      /* blind_rotation_basis_bits */
   uint32_t br_len;       /* ceil(bits(Q) / br_bits) (Basis::new, algebra/src/decompose_basis.rs:29-40) */
   uint32_t ks_bits;      /* key_switching_basis_bits */
   uint32_t ks_len;       /* ceil(bits(Q) / ks_bits) */
   uint32_t ring_ternary; /* ring secret key: 1 ternary, 0 binary */
+  uint32_t lwe_ternary;  /* LWE secret key: 1 ternary (HB_FIELD_DEFAULT_U32 only; LWESecretKeyType,
+                            fhe_core/src/secret_key.rs:12-18), 0 binary */
   double lwe_noise_std;
   double ring_noise_std;
   double ks_noise_std;

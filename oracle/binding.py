@@ -16,20 +16,36 @@ LIB_PATH = os.path.join(HERE, "libhb_oracle.so")
 
 FIELD_BABYBEAR = 0
 FIELD_GOLDILOCKS = 1
+FIELD_DEFAULT_U32 = 2
 
 PRESET_BABYBEAR = 0
 PRESET_GOLDILOCKS = 1
 PRESET_ZAMA = 2
+PRESET_DEFAULT_TERNARY = 3
+PRESET_CUSTOM_TERNARY = 4
 PRESET_NAMES = {
     PRESET_BABYBEAR: "BABYBEAR_BINARY_128_BITS",
     PRESET_GOLDILOCKS: "GOLDILOCKS_BINARY_128_BITS",
     PRESET_ZAMA: "ZAMA_BINARY_128_BITS",
+    PRESET_DEFAULT_TERNARY: "DEFAULT_TERNARY_128_BITS",
+    PRESET_CUSTOM_TERNARY: "CUSTOM_TERNARY_128_BITS",
 }
+
+# Key sets the tests use: the presets, plus CUSTOM_TERNARY_128_BITS with a ternary LWE key (no
+# reference preset configures one; TernaryBlindRotationKey,
+# fhe_core/src/blind_rotation/rlwe/ternary.rs, serves it).
+SET_TERNARY_LWE = 100
+SET_NAMES = dict(PRESET_NAMES)
+SET_NAMES[SET_TERNARY_LWE] = "CUSTOM_TERNARY_128_BITS_TERNARY_LWE_KEY"
+# Sets with n' = next_pow2(n) < N on the other two fields (key switching in N/n' chunks).
+SET_GOLDILOCKS_N500 = 101
+SET_BABYBEAR_N300 = 102
 
 GATES = {"nand": 0, "and": 1, "or": 2, "nor": 3, "xor": 4, "xnor": 5, "majority": 6,
          "not": 7, "mux": 8}
 
-MODULUS = {FIELD_BABYBEAR: 0x78000001, FIELD_GOLDILOCKS: 0xFFFFFFFF00000001}
+MODULUS = {FIELD_BABYBEAR: 0x78000001, FIELD_GOLDILOCKS: 0xFFFFFFFF00000001,
+           FIELD_DEFAULT_U32: 132120577}
 
 
 class OrcParams(ctypes.Structure):
@@ -42,6 +58,7 @@ class OrcParams(ctypes.Structure):
         ("ks_bits", ctypes.c_uint32),
         ("ks_len", ctypes.c_uint32),
         ("ring_ternary", ctypes.c_uint32),
+        ("lwe_ternary", ctypes.c_uint32),
         ("lwe_noise_std", ctypes.c_double),
         ("ring_noise_std", ctypes.c_double),
         ("ks_noise_std", ctypes.c_double),
@@ -105,9 +122,24 @@ def preset(pid):
     return p
 
 
+def params(set_id):
+    """Parameters of a key set (SET_NAMES)."""
+    if set_id == SET_TERNARY_LWE:
+        p = preset(PRESET_CUSTOM_TERNARY)
+        p.lwe_ternary = 1
+        return p
+    if set_id in (SET_GOLDILOCKS_N500, SET_BABYBEAR_N300):
+        p = preset(PRESET_GOLDILOCKS if set_id == SET_GOLDILOCKS_N500 else PRESET_BABYBEAR)
+        p.lwe_dim = 500 if set_id == SET_GOLDILOCKS_N500 else 300
+        return p
+    return preset(set_id)
+
+
 def sizes(p):
     N, n, L, Lks = p.ring_dim, p.lwe_dim, p.br_len, p.ks_len
-    return {"lwe_sk": n, "ring_sk": N, "bsk": n * 2 * L * 2 * N, "ksk": Lks * 2 * N, "lwe": n + 1}
+    pairs = 2 if p.lwe_ternary else 1
+    return {"lwe_sk": n, "ring_sk": N, "bsk": n * pairs * 2 * L * 2 * N, "ksk": Lks * 2 * N,
+            "lwe": n + 1}
 
 
 class Keys:

@@ -106,13 +106,21 @@ struct Gold {
   static T from_u64(uint64_t v) { return v; }  // Goldilocks::new stores the word unchanged
 };
 
-// BabyBear Q = 2^31 - 2^27 + 1 (algebra/src/modulus/baby_bear/mod.rs:11). The reference stores
-// Montgomery form; every operation on the path returns canonical residues, so the oracle works on
-// canonical values directly.
-struct Baby {
+// 32-bit prime fields with canonical words:
+//  - BabyBear Q = 2^31 - 2^27 + 1 (algebra/src/modulus/baby_bear/mod.rs:11). The reference stores
+//    Montgomery form; every operation on the path returns canonical residues, so the oracle works
+//    on canonical values directly. bits(Q) = 31 (algebra/src/baby_bear/mod.rs:73-79).
+//  - DefaultFieldU32 Q = 132120577 = 2^27 - 2^21 + 1 (fhe_core/src/parameter.rs:286-290): a
+//    derived Barrett field storing the plain residue (algebra_derive/src/field.rs:91-120) with the
+//    usual add/sub/neg reductions (algebra_derive/src/ops.rs:25-113); bits(Q) = 27, the bit length
+//    of the modulus (algebra/src/modulus/barrett/internal_macros.rs:74-76). Its lazy FheField
+//    products (algebra_derive/src/fhe_field.rs:31-42) only feed inverse transforms, whose outputs
+//    are canonical, so exact products give the same coefficients.
+template <uint32_t PP, int BB>
+struct Prime32 {
   using T = uint32_t;
-  static constexpr T P = 0x78000001U;
-  static constexpr int BITS = 31;  // algebra/src/baby_bear/mod.rs:73-79
+  static constexpr T P = PP;
+  static constexpr int BITS = BB;
 
   static T canon(T x) { return x % P; }
   static T add(T a, T b) {
@@ -133,6 +141,13 @@ struct Baby {
   static T value(T a) { return a; }
   static T from_u64(uint64_t v) { return (T)(v % P); }
 };
+using Baby = Prime32<0x78000001U, 31>;
+using Dflt = Prime32<0x07E00001U, 27>;
+
+// bits(Q) of a field id (the decomposition length is ceil(bits(Q) / basis bits)).
+inline int field_bits(int field_id) {
+  return field_id == ORC_FIELD_GOLDILOCKS ? 64 : field_id == ORC_FIELD_BABYBEAR ? 31 : 27;
+}
 
 template <class F>
 typename F::T fpow(typename F::T b, uint64_t e) {
@@ -333,31 +348,73 @@ typename F::T uniform(uint64_t seed, uint64_t stream, uint64_t k) {
   return (typename F::T)(prg(seed, stream, k) % (uint64_t)F::P);
 }
 
+// random_with_gaussian draws error polynomials from sample_cbd_field_vec instead of the Gaussian
+// when the sampler has mean 0 and sigma exactly 3.2 (algebra/src/random.rs:91-92,
+// algebra/src/polynomial/univariate/native_polynomial.rs:232-246).
+inline bool cbd_enabled(double sigma) { return sigma == 3.2; }
+
+// sample_cbd_field_vec (algebra/src/utils/sample.rs:54-75): six random bytes (here the low six
+// bytes of one PRG word), the third and sixth masked to 5 bits; a and b are the popcounts of the
+// first and last three. For a < b the reference evaluates `modulus - (a - b)` with a u32
+// subtraction that wraps in release builds, so the value is Field::new of that wrapped word in
+// the field's word width: b - a for the 32-bit fields, P - (2^32 - (b - a)) for Goldilocks.
+template <class F>
+typename F::T cbd(uint64_t seed, uint64_t stream, uint64_t coeff) {
+  using T = typename F::T;
+  const uint64_t r = prg(seed, stream, coeff);
+  auto pc = [](uint64_t x) { return (uint32_t)__builtin_popcountll(x); };
+  const uint32_t a = pc(r & 0xFF) + pc((r >> 8) & 0xFF) + pc((r >> 16) & 0x1F);
+  const uint32_t b = pc((r >> 24) & 0xFF) + pc((r >> 32) & 0xFF) + pc((r >> 40) & 0x1F);
+  const uint32_t d = a - b;  // wraps when a < b
+  if (a >= b) return (T)d;
+  return F::from_u64((uint64_t)(T)((T)F::P - (T)d));
+}
+
+// One error coefficient of an RLWE zero sample.
+template <class F>
+typename F::T error_coeff(uint64_t seed, uint64_t stream, uint64_t coeff, double sigma) {
+  return cbd_enabled(sigma) ? cbd<F>(seed, stream, coeff) : gaussian<F>(seed, stream, coeff, sigma);
+}
+
 // ------------------------------------------------------------------------------------------
 // Parameters
 // ------------------------------------------------------------------------------------------
 
 struct Dims {
   uint32_t N, logN, n, bits, len, ks_bits, ks_len;
+  uint32_t ks_n, ks_logn, chunks;  // key switch: n' = next_pow2(n), N / n' key chunks
+  uint32_t pairs;                  // RGSWs per LWE key coefficient: 1 binary, 2 ternary
 };
 
 bool dims_of(const orc_params *p, Dims &d) {
   if (!p) return false;
+  if (p->field_id != ORC_FIELD_GOLDILOCKS && p->field_id != ORC_FIELD_BABYBEAR &&
+      p->field_id != ORC_FIELD_DEFAULT_U32)
+    return false;
   d.N = p->ring_dim;
   d.n = p->lwe_dim;
   if (d.N < 2 || (d.N & (d.N - 1)) || d.N > 4096) return false;
   d.logN = 0;
   while ((1u << d.logN) < d.N) ++d.logN;
   if (d.n == 0 || d.n > d.N) return false;
-  // key_switch_for_rlwe requires next_pow2(n) == N for the single-chunk path the paper sets take
-  uint32_t np2 = 1;
-  while (np2 < d.n) np2 <<= 1;
-  if (np2 != d.N) return false;
+  // KeySwitchingRLWEKey::generate: extended_lwe_dimension = next_pow2(n) <= N, and the ring key
+  // splits into N / n' chunks when it is smaller (fhe_core/src/key_switch/rlwe.rs:40-43,79-108)
+  d.ks_n = 1;
+  d.ks_logn = 0;
+  while (d.ks_n < d.n) {
+    d.ks_n <<= 1;
+    ++d.ks_logn;
+  }
+  d.chunks = d.N / d.ks_n;
+  // Ternary LWE keys take TernaryBlindRotationKey (fhe_core/src/blind_rotation/rlwe/ternary.rs),
+  // whose NTT-domain monomial is marked incompatible with BabyBear and Goldilocks there (:80).
+  if (p->lwe_ternary > 1 || (p->lwe_ternary && p->field_id != ORC_FIELD_DEFAULT_U32)) return false;
+  d.pairs = p->lwe_ternary ? 2 : 1;
   d.bits = p->br_bits;
   d.len = p->br_len;
   d.ks_bits = p->ks_bits;
   d.ks_len = p->ks_len;
-  int fb = p->field_id == ORC_FIELD_GOLDILOCKS ? 64 : 31;
+  int fb = field_bits(p->field_id);
   auto want = [&](uint32_t b) { return (uint32_t)((fb + (int)b - 1) / (int)b); };
   if (d.bits == 0 || d.bits > 16 || d.len != want(d.bits)) return false;
   if (d.ks_bits == 0 || d.ks_bits > 16 || d.ks_len != want(d.ks_bits)) return false;
@@ -388,7 +445,7 @@ void rlwe_zero_sample(const Ntt<F> &ntt, const typename F::T *key_ntt, uint64_t 
   uint32_t N = ntt.n;
   for (uint32_t k = 0; k < N; ++k) a[k] = uniform<F>(seed, stream_a, k);
   negacyclic_mul<F>(ntt, a, key_ntt, b);
-  for (uint32_t k = 0; k < N; ++k) b[k] = F::add(b[k], gaussian<F>(seed, stream_e, k, sigma));
+  for (uint32_t k = 0; k < N; ++k) b[k] = F::add(b[k], error_coeff<F>(seed, stream_e, k, sigma));
 }
 
 template <class F>
@@ -397,45 +454,51 @@ void keygen(const orc_params *p, const Dims &d, uint64_t seed, typename F::T *lw
   using T = typename F::T;
   const uint32_t N = d.N, n = d.n;
   const Ntt<F> &ntt = ntt_table<F>(d.logN);
-  // sample_binary_field_vec (algebra/src/utils/sample.rs:6-27)
-  for (uint32_t i = 0; i < n; ++i) lwe_sk[i] = (T)(prg(seed, stream_id(TAG_LWE_SK, 0, 0, 0, 0), i) & 1);
-  // sample_ternary_field_vec / random_with_binary (algebra/src/utils/sample.rs:30-51)
+  // sample_binary_field_vec / sample_ternary_field_vec (algebra/src/utils/sample.rs:6-51;
+  // fhe_core/src/secret_key.rs:60-63): a bit, or {0, 0, 1, -1}[r & 3]
+  const T tern[4] = {0, 0, 1, (T)(F::P - 1)};
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint64_t r = prg(seed, stream_id(TAG_LWE_SK, 0, 0, 0, 0), i);
+    lwe_sk[i] = d.pairs == 2 ? tern[r & 3] : (T)(r & 1);
+  }
+  // random_with_ternary / random_with_binary (fhe_core/src/secret_key.rs:74-79)
   for (uint32_t k = 0; k < N; ++k) {
     uint64_t r = prg(seed, stream_id(TAG_RING_SK, 0, 0, 0, 0), k);
-    if (p->ring_ternary) {
-      const T tbl[4] = {0, 0, 1, (T)(F::P - 1)};
-      ring_sk[k] = tbl[r & 3];
-    } else {
-      ring_sk[k] = (T)(r & 1);
-    }
+    ring_sk[k] = p->ring_ternary ? tern[r & 3] : (T)(r & 1);
   }
   std::vector<T> z_ntt(ring_sk, ring_sk + N);
   ntt.forward(z_ntt.data());
 
+  // Blind-rotation key: per LWE key coefficient one NTTRGSW of s_i (binary,
+  // fhe_core/src/blind_rotation/rlwe/binary.rs:207-239), or the pair (RGSW(s_i == 1),
+  // RGSW(s_i == -1)) (ternary, fhe_core/src/blind_rotation/rlwe/ternary.rs:123-183). Layout
+  // [i][pair][part][j][ab][N]; pair 1 draws from streams part + 2.
   const uint32_t L = d.len;
   const size_t row = 2 * (size_t)N;            // one RLWE (a, b)
   const size_t entry = 2 * (size_t)L * row;    // one RGSW = (c_neg_s_m, c_m)
   auto work = [&](uint32_t i0, uint32_t i1) {
     for (uint32_t i = i0; i < i1; ++i) {
-      const bool one = lwe_sk[i] != 0;
-      T basis_pow = 1;
-      for (uint32_t j = 0; j < L; ++j) {
-        for (uint32_t part = 0; part < 2; ++part) {
-          T *a = bsk + (size_t)i * entry + ((size_t)part * L + j) * row;
-          T *b = a + N;
-          rlwe_zero_sample<F>(ntt, z_ntt.data(), seed, stream_id(TAG_BSK, i, part, j, 0),
-                              stream_id(TAG_BSK, i, part, j, 1), p->ring_noise_std, a, b);
-          if (one && part == 0) {
-            // generate_random_neg_secret_sample: every NTT slot of a += B^j, i.e. a[0] += B^j
-            // (lattice/src/gadget/rlwe.rs:526-551)
-            a[0] = F::add(a[0], basis_pow);
-          } else if (one && part == 1) {
-            // generate_random_value_sample: e[0] += B^j before the transform (lattice/src/rlwe.rs:1233-1252)
-            b[0] = F::add(b[0], basis_pow);
+      for (uint32_t pair = 0; pair < d.pairs; ++pair) {
+        const bool one = d.pairs == 1 ? lwe_sk[i] != 0 : lwe_sk[i] == (pair == 0 ? (T)1 : (T)(F::P - 1));
+        T basis_pow = 1;
+        for (uint32_t j = 0; j < L; ++j) {
+          for (uint32_t part = 0; part < 2; ++part) {
+            T *a = bsk + ((size_t)i * d.pairs + pair) * entry + ((size_t)part * L + j) * row;
+            T *b = a + N;
+            rlwe_zero_sample<F>(ntt, z_ntt.data(), seed, stream_id(TAG_BSK, i, part + 2 * pair, j, 0),
+                                stream_id(TAG_BSK, i, part + 2 * pair, j, 1), p->ring_noise_std, a, b);
+            if (one && part == 0) {
+              // generate_random_neg_secret_sample: every NTT slot of a += B^j, i.e. a[0] += B^j
+              // (lattice/src/gadget/rlwe.rs:526-551)
+              a[0] = F::add(a[0], basis_pow);
+            } else if (one && part == 1) {
+              // generate_random_value_sample: e[0] += B^j before the transform (lattice/src/rlwe.rs:1233-1252)
+              b[0] = F::add(b[0], basis_pow);
+            }
           }
+          // basis_power = lazy_new(basis_power.value() * basis) (lattice/src/gadget/rlwe.rs:518,546)
+          basis_pow = (T)((uint64_t)basis_pow << d.bits);
         }
-        // basis_power = lazy_new(basis_power.value() * basis) (lattice/src/gadget/rlwe.rs:518,546)
-        basis_pow = (T)((uint64_t)basis_pow << d.bits);
       }
     }
   };
@@ -449,21 +512,27 @@ void keygen(const orc_params *p, const Dims &d, uint64_t seed, typename F::T *lw
   }
   for (auto &th : pool) th.join();
 
-  // KeySwitchingRLWEKey::generate (fhe_core/src/key_switch/rlwe.rs:37-112), next_pow2(n) == N branch:
-  // row j encrypts z * B_ks^j under the extended LWE key [s, 0...].
-  std::vector<T> s_ext(N, 0);
+  // KeySwitchingRLWEKey::generate (fhe_core/src/key_switch/rlwe.rs:37-112): the LWE key padded to
+  // n' = next_pow2(n) words; one gadget RLWE of dimension n' per n'-word chunk z_c of the ring key
+  // (a single one, z itself, when n' == N). Row j of chunk c encrypts z_c * B_ks^j; layout
+  // [c][j][ab][n'].
+  const uint32_t M = d.ks_n;
+  const Ntt<F> &kntt = ntt_table<F>(d.ks_logn);
+  std::vector<T> s_ext(M, 0);
   for (uint32_t i = 0; i < n; ++i) s_ext[i] = lwe_sk[i];
-  ntt.forward(s_ext.data());
-  std::vector<T> zk(ring_sk, ring_sk + N);
+  kntt.forward(s_ext.data());
   const T basis_ks = F::from_u64(1ull << d.ks_bits);
-  for (uint32_t j = 0; j < d.ks_len; ++j) {
-    T *a = ksk + (size_t)j * row;
-    T *b = a + N;
-    rlwe_zero_sample<F>(ntt, s_ext.data(), seed, stream_id(TAG_KSK, 0, 0, j, 0),
-                        stream_id(TAG_KSK, 0, 0, j, 1), p->ks_noise_std, a, b);
-    for (uint32_t k = 0; k < N; ++k) b[k] = F::add(b[k], zk[k]);
-    if (j + 1 < d.ks_len)
-      for (uint32_t k = 0; k < N; ++k) zk[k] = F::mul(zk[k], basis_ks);
+  for (uint32_t c = 0; c < d.chunks; ++c) {
+    std::vector<T> zk(ring_sk + (size_t)c * M, ring_sk + (size_t)(c + 1) * M);
+    for (uint32_t j = 0; j < d.ks_len; ++j) {
+      T *a = ksk + ((size_t)c * d.ks_len + j) * 2 * M;
+      T *b = a + M;
+      rlwe_zero_sample<F>(kntt, s_ext.data(), seed, stream_id(TAG_KSK, c, 0, j, 0),
+                          stream_id(TAG_KSK, c, 0, j, 1), p->ks_noise_std, a, b);
+      for (uint32_t k = 0; k < M; ++k) b[k] = F::add(b[k], zk[k]);
+      if (j + 1 < d.ks_len)
+        for (uint32_t k = 0; k < M; ++k) zk[k] = F::mul(zk[k], basis_ks);
+    }
   }
 }
 
@@ -523,8 +592,8 @@ template <class F>
 struct EvalKey {
   using T = typename F::T;
   Dims d;
-  std::vector<T> bsk_ntt;  // [i][part][j][ab][N] in this oracle's NTT domain
-  std::vector<T> ksk_ntt;  // [j][ab][N]
+  std::vector<T> bsk_ntt;  // [i][pair][part][j][ab][N] in this oracle's NTT domain
+  std::vector<T> ksk_ntt;  // [c][j][ab][n'] (n'-point transforms)
 };
 
 template <class F>
@@ -533,7 +602,7 @@ EvalKey<F> *make_eval(const Dims &d, const typename F::T *bsk, const typename F:
   auto *ek = new EvalKey<F>();
   ek->d = d;
   const Ntt<F> &ntt = ntt_table<F>(d.logN);
-  size_t polys = (size_t)d.n * 2 * d.len * 2;
+  size_t polys = (size_t)d.n * d.pairs * 2 * d.len * 2;
   ek->bsk_ntt.assign(bsk, bsk + polys * d.N);
   int nt = std::max(1, threads);
   std::vector<std::thread> pool;
@@ -546,8 +615,10 @@ EvalKey<F> *make_eval(const Dims &d, const typename F::T *bsk, const typename F:
     });
   }
   for (auto &th : pool) th.join();
-  ek->ksk_ntt.assign(ksk, ksk + (size_t)d.ks_len * 2 * d.N);
-  for (size_t q = 0; q < (size_t)d.ks_len * 2; ++q) ntt.forward(ek->ksk_ntt.data() + q * d.N);
+  const Ntt<F> &kntt = ntt_table<F>(d.ks_logn);
+  const size_t kpolys = (size_t)d.chunks * d.ks_len * 2;
+  ek->ksk_ntt.assign(ksk, ksk + kpolys * d.ks_n);
+  for (size_t q = 0; q < kpolys; ++q) kntt.forward(ek->ksk_ntt.data() + q * d.ks_n);
   return ek;
 }
 
@@ -678,33 +749,113 @@ void blind_rotate(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T 
   }
 }
 
+// NTT of the monomial c * X^deg, deg in [0, 2N) (X^N = -1), as
+// MonomialNTT::transform_monomial / transform_coeff_neg_one_monomial
+// (algebra/src/transformation/concrete.rs:63-84) produce it.
+template <class F>
+void monomial_ntt(const Ntt<F> &ntt, typename F::T c, uint32_t deg, typename F::T *out) {
+  const uint32_t N = ntt.n;
+  std::fill(out, out + N, (typename F::T)0);
+  if (deg < N)
+    out[deg] = c;
+  else
+    out[deg - N] = F::neg(c);
+  ntt.forward(out);
+}
+
+// TernaryBlindRotationKey::blind_rotate (fhe_core/src/blind_rotation/rlwe/ternary.rs:26-119): the
+// LUT rotated by an NTT product with X^-b; per step with a_i != 0 the evaluation key
+// RGSW(s_i == 1) + RGSW(s_i == -1) * NTT(-X^-a_i) (lattice/src/rgsw.rs:321-338) multiplies
+// E = (X^a_i - 1) * ACC, computed through the NTT, and ACC += the product. The fields this path
+// accepts keep canonical words, so the reference's representation-level operations are the
+// canonical ones.
+template <class F>
+void blind_rotate_ternary(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T *lut_in,
+                          uint32_t steps, typename F::T *acc_a, typename F::T *acc_b) {
+  using T = typename F::T;
+  const Dims &d = ek.d;
+  const uint32_t N = d.N;
+  const Ntt<F> &ntt = ntt_table<F>(d.logN);
+  std::vector<T> lut(lut_in, lut_in + N), mono(N), t(N);
+  const uint32_t b = ms[d.n];
+  if (b != 0) {  // ternary.rs:43-56
+    monomial_ntt<F>(ntt, (T)1, 2 * N - b, mono.data());
+    ntt.forward(lut.data());
+    for (uint32_t k = 0; k < N; ++k) lut[k] = F::mul(lut[k], mono[k]);
+    ntt.inverse(lut.data());
+  }
+  std::fill(acc_a, acc_a + N, (T)0);
+  std::copy(lut.begin(), lut.end(), acc_b);
+  const size_t rgsw = (size_t)2 * d.len * 2 * N;
+  std::vector<T> evk(rgsw), ea(N), eb(N);
+  for (uint32_t i = 0; i < d.n && i < steps; ++i) {
+    const uint32_t ai = ms[i];
+    if (ai == 0) continue;  // ternary.rs:73
+    // evaluation_key = RGSW_0 + RGSW_1 * NTT(-X^(2N - a_i)) (ternary.rs:78-89)
+    monomial_ntt<F>(ntt, (T)(F::P - 1), 2 * N - ai, mono.data());
+    const T *k0 = ek.bsk_ntt.data() + (size_t)i * 2 * rgsw;
+    const T *k1 = k0 + rgsw;
+    for (size_t q = 0; q < rgsw; ++q) evk[q] = F::add(k0[q], F::mul(k1[q], mono[q % N]));
+    // external_product = (X^a_i - 1) * ACC through the NTT (ternary.rs:91-103)
+    monomial_ntt<F>(ntt, (T)1, ai, mono.data());
+    for (int part = 0; part < 2; ++part) {
+      const T *y = part == 0 ? acc_a : acc_b;
+      T *e = part == 0 ? ea.data() : eb.data();
+      std::copy(y, y + N, t.data());
+      ntt.forward(t.data());
+      for (uint32_t k = 0; k < N; ++k) t[k] = F::mul(t[k], mono[k]);
+      ntt.inverse(t.data());
+      for (uint32_t k = 0; k < N; ++k) e[k] = F::sub(t[k], y[k]);
+    }
+    external_product<F>(ntt, d.bits, d.len, evk.data(), ea.data(), eb.data());
+    for (uint32_t k = 0; k < N; ++k) {  // ternary.rs:114
+      acc_a[k] = F::add(acc_a[k], ea[k]);
+      acc_b[k] = F::add(acc_b[k], eb[k]);
+    }
+  }
+}
+
 // KeySwitchingRLWEKey::key_switch_for_rlwe (fhe_core/src/key_switch/rlwe.rs:115-137) with
 // key_switch_inner (SubAMulS, :250-286) and extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402).
+// With n' = next_pow2(n) < N the accumulator's a is first negated at 0 and reversed on [1, N),
+// then the same on every n'-word chunk (:123-131), and each chunk is switched with its own key.
 template <class F>
 void key_switch(const EvalKey<F> &ek, const typename F::T *acc_a, const typename F::T *acc_b,
                 typename F::T *out) {
   using T = typename F::T;
   const Dims &d = ek.d;
-  const uint32_t N = d.N;
-  const Ntt<F> &ntt = ntt_table<F>(d.logN);
-  std::vector<T> ia(N, 0), ib(N, F::canon(acc_b[0]));  // NTTRLWE(0, [b0; N])
-  std::vector<T> poly(N), digit(N);
-  // sub_assign_gadget_rlwe_mul_polynomial_inplace_fast (lattice/src/rlwe.rs:1147-1166): negate, then add
-  for (uint32_t k = 0; k < N; ++k) poly[k] = F::neg_ref(acc_a[k]);
-  for (uint32_t j = 0; j < d.ks_len; ++j) {
-    decompose_step<F>(poly.data(), digit.data(), N, d.ks_bits);
-    ntt.forward(digit.data());
-    const T *ka = ek.ksk_ntt.data() + (size_t)j * 2 * N;
-    const T *kb = ka + N;
-    for (uint32_t k = 0; k < N; ++k) {
-      ia[k] = F::add(ia[k], F::mul(digit[k], ka[k]));
-      ib[k] = F::add(ib[k], F::mul(digit[k], kb[k]));
+  const uint32_t N = d.N, M = d.ks_n;
+  const Ntt<F> &ntt = ntt_table<F>(d.ks_logn);
+  std::vector<T> a(acc_a, acc_a + N);
+  if (M != N) {
+    a[0] = F::neg_ref(a[0]);
+    std::reverse(a.begin() + 1, a.end());
+    for (uint32_t c = 0; c < d.chunks; ++c) {
+      T *ch = a.data() + (size_t)c * M;
+      ch[0] = F::neg_ref(ch[0]);
+      std::reverse(ch + 1, ch + M);
+    }
+  }
+  std::vector<T> ia(M, 0), ib(M, F::canon(acc_b[0]));  // NTTRLWE(0, [b0; n'])
+  std::vector<T> poly(M), digit(M);
+  for (uint32_t c = 0; c < d.chunks; ++c) {
+    // sub_assign_gadget_rlwe_mul_polynomial_inplace_fast (lattice/src/rlwe.rs:1147-1166): negate, then add
+    for (uint32_t k = 0; k < M; ++k) poly[k] = F::neg_ref(a[(size_t)c * M + k]);
+    for (uint32_t j = 0; j < d.ks_len; ++j) {
+      decompose_step<F>(poly.data(), digit.data(), M, d.ks_bits);
+      ntt.forward(digit.data());
+      const T *ka = ek.ksk_ntt.data() + ((size_t)c * d.ks_len + j) * 2 * M;
+      const T *kb = ka + M;
+      for (uint32_t k = 0; k < M; ++k) {
+        ia[k] = F::add(ia[k], F::mul(digit[k], ka[k]));
+        ib[k] = F::add(ib[k], F::mul(digit[k], kb[k]));
+      }
     }
   }
   ntt.inverse(ia.data());
   ntt.inverse(ib.data());
   out[0] = ia[0];
-  for (uint32_t k = 1; k < d.n; ++k) out[k] = F::neg_ref(ia[N - k]);
+  for (uint32_t k = 1; k < d.n; ++k) out[k] = F::neg_ref(ia[M - k]);
   out[d.n] = ib[0];
 }
 
@@ -717,7 +868,10 @@ void bootstrap(const EvalKey<F> &ek, const typename F::T *c, const typename F::T
   std::vector<uint32_t> ms(d.n + 1);
   modswitch<F>(d, c, ms.data());
   std::vector<T> acc_a(d.N), acc_b(d.N);
-  blind_rotate<F>(ek, ms.data(), lut, d.n, acc_a.data(), acc_b.data());
+  if (d.pairs == 2)
+    blind_rotate_ternary<F>(ek, ms.data(), lut, d.n, acc_a.data(), acc_b.data());
+  else
+    blind_rotate<F>(ek, ms.data(), lut, d.n, acc_a.data(), acc_b.data());
   acc_b[0] = F::add_ref(acc_b[0], (T)((uint64_t)F::P >> 3));  // evaluate.rs:52
   key_switch<F>(ek, acc_a.data(), acc_b.data(), out);
 }
@@ -842,6 +996,20 @@ int orc_params_preset(int preset, orc_params *out) {
       out->ring_noise_std = 2.3 * (double)(1ULL << 37);
       out->ks_noise_std = 2.9 * (double)(1ULL << 45);
       return 0;
+    case 3:  // DEFAULT_TERNARY_128_BITS_PARAMETERS (tfhe/src/bfhe/parameters.rs:7-23)
+    case 4:  // CUSTOM_TERNARY_128_BITS_PARAMETERS (tfhe/src/bfhe/parameters.rs:26-42)
+      // Both sets name their ring "ternary" but configure binary LWE and ring keys.
+      out->field_id = ORC_FIELD_DEFAULT_U32;
+      out->lwe_dim = preset == 3 ? 1024 : 512;
+      out->ring_ternary = 0;
+      out->br_bits = preset == 3 ? 3 : 7;
+      out->br_len = preset == 3 ? 9 : 4;
+      out->ks_bits = preset == 3 ? 1 : 7;
+      out->ks_len = preset == 3 ? 27 : 4;
+      out->lwe_noise_std = 3.20;
+      out->ring_noise_std = 3.20 * 2.0;
+      out->ks_noise_std = 3.2 * 2.0;
+      return 0;
     default:
       return -1;
   }
@@ -856,6 +1024,9 @@ uint64_t orc_prg(uint64_t seed, uint64_t stream, uint64_t ctr) { return prg(seed
       BODY;                                                    \
     } else if ((p)->field_id == ORC_FIELD_BABYBEAR) {          \
       using F = Baby;                                          \
+      BODY;                                                    \
+    } else if ((p)->field_id == ORC_FIELD_DEFAULT_U32) {       \
+      using F = Dflt;                                          \
       BODY;                                                    \
     } else {                                                   \
       return -1;                                               \
@@ -902,7 +1073,7 @@ int orc_decrypt(const orc_params *p, const void *lwe_sk, const void *lwe, size_t
 struct orc_eval {
   orc_params p;
   Dims d;
-  void *ek;  // EvalKey<Gold> or EvalKey<Baby>
+  void *ek;  // EvalKey<F> of the parameter set's field
 };
 
 int orc_eval_create(const orc_params *p, const void *bsk, const void *ksk, int threads, orc_eval **out) {
@@ -924,8 +1095,10 @@ void orc_eval_free(orc_eval *e) {
   if (!e) return;
   if (e->p.field_id == ORC_FIELD_GOLDILOCKS)
     delete (EvalKey<Gold> *)e->ek;
-  else
+  else if (e->p.field_id == ORC_FIELD_BABYBEAR)
     delete (EvalKey<Baby> *)e->ek;
+  else
+    delete (EvalKey<Dflt> *)e->ek;
   delete e;
 }
 
@@ -997,14 +1170,17 @@ int orc_blind_rotate(const orc_params *p, const void *bsk, const void *c, const 
     ek->d = dd;
     const Ntt<F> &ntt = ntt_table<F>(d.logN);
     uint32_t used = std::min(steps, d.n);
-    size_t entry = (size_t)2 * d.len * 2 * d.N;
+    size_t entry = (size_t)d.pairs * 2 * d.len * 2 * d.N;
     ek->bsk_ntt.assign((const T *)bsk, (const T *)bsk + used * entry);
-    for (size_t q = 0; q < used * (size_t)2 * d.len * 2; ++q)
+    for (size_t q = 0; q < used * (size_t)d.pairs * 2 * d.len * 2; ++q)
       ntt.forward(ek->bsk_ntt.data() + q * d.N);
     std::vector<uint32_t> ms(d.n + 1);
     modswitch<F>(d, (const T *)c, ms.data());
     T *acc = (T *)acc_out;
-    blind_rotate<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N);
+    if (d.pairs == 2)
+      blind_rotate_ternary<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N);
+    else
+      blind_rotate<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N);
     for (uint32_t k = 0; k < 2 * d.N; ++k) acc[k] = F::canon(acc[k]);
   });
   return 0;

@@ -2,8 +2,9 @@
  * hb_oracle.h -- TEST INFRASTRUCTURE ONLY.
  *
  * CPU restatement of HasteBoots' TFHE gate-bootstrapping path (tfhe crate evaluator,
- * fhe_core modulus switch / binary blind rotation / RLWE key switching, lattice RLWE/RGSW
- * external product, algebra Goldilocks/BabyBear arithmetic and unsigned gadget decomposition).
+ * fhe_core modulus switch / binary and ternary blind rotation / RLWE key switching, lattice
+ * RLWE/RGSW external product, algebra Goldilocks/BabyBear/DefaultFieldU32 arithmetic and unsigned
+ * gadget decomposition).
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load this library,
  * and only as the checker. The product (hasteboots_b200/, libhb_gpu.so) never links it.
@@ -17,7 +18,7 @@
  * noise < Q/16). Bit-exactness with the live Rust binary is therefore "parity unpinned".
  *
  * All buffers hold canonical little-endian field values: uint64_t words for Goldilocks,
- * uint32_t words for BabyBear.
+ * uint32_t words for BabyBear and DefaultFieldU32 (Q = 132120577).
  */
 #ifndef HB_ORACLE_H
 #define HB_ORACLE_H
@@ -29,7 +30,7 @@
 extern "C" {
 #endif
 
-enum { ORC_FIELD_BABYBEAR = 0, ORC_FIELD_GOLDILOCKS = 1 };
+enum { ORC_FIELD_BABYBEAR = 0, ORC_FIELD_GOLDILOCKS = 1, ORC_FIELD_DEFAULT_U32 = 2 };
 
 enum {
   ORC_GATE_NAND = 0,
@@ -43,32 +44,36 @@ enum {
   ORC_GATE_MUX = 8
 };
 
-/* Mirrors fhe_core::ConstParameters (fhe_core/src/parameter.rs:81-107) restricted to the
- * binary-LWE-key / RLWE-bootstrapping branch that the paper parameter sets use. */
+/* Mirrors fhe_core::ConstParameters (fhe_core/src/parameter.rs:81-107) for RLWE bootstrapping
+ * with the RLWE key switch. */
 typedef struct orc_params {
   int32_t field_id;      /* ORC_FIELD_* */
   uint32_t ring_dim;     /* N */
-  uint32_t lwe_dim;      /* n */
+  uint32_t lwe_dim;      /* n, next_pow2(n) <= N */
   uint32_t br_bits;      /* blind_rotation_basis_bits */
   uint32_t br_len;       /* ceil(bits(Q)/br_bits) */
   uint32_t ks_bits;      /* key_switching_basis_bits */
   uint32_t ks_len;       /* ceil(bits(Q)/ks_bits) */
   uint32_t ring_ternary; /* 1: ternary ring key, 0: binary */
+  uint32_t lwe_ternary;  /* 1: ternary LWE key (DefaultFieldU32 only), 0: binary */
   double lwe_noise_std;
   double ring_noise_std;
   double ks_noise_std;
 } orc_params;
 
-/* 0: BABYBEAR_BINARY_128_BITS, 1: GOLDILOCKS_BINARY_128_BITS, 2: ZAMA_BINARY_128_BITS
- * (tfhe/src/bfhe/parameters.rs:45-117). Returns 0 or -1 for an unknown id. */
+/* 0: BABYBEAR_BINARY_128_BITS, 1: GOLDILOCKS_BINARY_128_BITS, 2: ZAMA_BINARY_128_BITS,
+ * 3: DEFAULT_TERNARY_128_BITS, 4: CUSTOM_TERNARY_128_BITS (tfhe/src/bfhe/parameters.rs:7-117).
+ * Returns 0 or -1 for an unknown id. */
 int orc_params_preset(int preset, orc_params *out);
 
 /* The splitmix-style counter PRG that defines the project's seeded key convention. */
 uint64_t orc_prg(uint64_t seed, uint64_t stream, uint64_t ctr);
 
 /* Key generation from a seed. Output sizes (words): lwe_sk n, ring_sk N,
- * bsk n*2*br_len*2*N (layout [i][part: 0=c_neg_s_m, 1=c_m][j][0=a,1=b][k]),
- * ksk ks_len*2*N (layout [j][0=a,1=b][k]). All coefficient domain. */
+ * bsk n*pairs*2*br_len*2*N (layout [i][pair][part: 0=c_neg_s_m, 1=c_m][j][0=a,1=b][k]; one pair
+ * for a binary LWE key, two -- RGSW(s_i == 1), RGSW(s_i == -1) -- for a ternary one),
+ * ksk ks_len*2*N (layout [c][j][0=a,1=b][k < n'], n' = next_pow2(n), c < N/n'). All coefficient
+ * domain. */
 int orc_keygen(const orc_params *p, uint64_t seed, void *lwe_sk, void *ring_sk, void *bsk,
                void *ksk, int threads);
 

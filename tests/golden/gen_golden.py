@@ -2,7 +2,9 @@
 
     python tests/golden/gen_golden.py
 
-For each parameter set (BABYBEAR / GOLDILOCKS / ZAMA _BINARY_128_BITS) with key seed 0 it records:
+For each key set (the BABYBEAR / GOLDILOCKS / ZAMA _BINARY_128_BITS and DEFAULT / CUSTOM
+_TERNARY_128_BITS presets, and CUSTOM_TERNARY_128_BITS with a ternary LWE key) with key seed 0 it
+records:
 SHA-256 digests of the secret keys, BSK and KSK (the project's seeded key convention); the input
 ciphertexts of the four NAND truth-table rows (encryption seed 0, sample indices 0..7); the oracle's
 NAND outputs. The BabyBear set also records every other gate, a caller-LUT bootstrap, the modulus
@@ -31,8 +33,8 @@ def digest(a):
 
 def main():
     out = {}
-    for pid, name in O.PRESET_NAMES.items():
-        p = O.preset(pid)
+    for pid, name in O.SET_NAMES.items():
+        p = O.params(pid)
         k = O.keygen(p, 0)
         out[f"{name}/sha_lwe_sk"] = np.array(digest(k.lwe_sk))
         out[f"{name}/sha_ring_sk"] = np.array(digest(k.ring_sk))

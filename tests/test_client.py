@@ -6,12 +6,14 @@ import os
 import numpy as np
 import pytest
 
+from conftest import ALL_SETS, hb_params_of
+
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_seed0.npz")
 
 
-@pytest.mark.parametrize("pid", [0, 1, 2])
+@pytest.mark.parametrize("pid", ALL_SETS)
 def test_product_keygen_matches_oracle(hb, oracle, oracle_keys, pid):
-    p = hb.Parameters.preset(pid)
+    p = hb_params_of(hb, pid)
     sk = hb.KeyGen.generate_secret_key(p, 0)
     bsk, ksk = sk.evaluation_key_material()
     k = oracle_keys(pid)
@@ -20,13 +22,21 @@ def test_product_keygen_matches_oracle(hb, oracle, oracle_keys, pid):
     assert (bsk == k.bsk).all()
     assert (ksk == k.ksk).all()
     g = np.load(GOLDEN)
-    name = oracle.PRESET_NAMES[pid]
+    name = oracle.SET_NAMES[pid]
     assert hashlib.sha256(bsk.tobytes()).hexdigest() == str(g[f"{name}/sha_bsk"])
 
 
-@pytest.mark.parametrize("pid", [0, 1, 2])
+@pytest.mark.parametrize("pid", [101, 102])
+def test_chunked_key_switching_key_matches_oracle(hb, oracle_keys, pid):
+    sk = hb.KeyGen.generate_secret_key(hb_params_of(hb, pid), 0)
+    bsk, ksk = sk.evaluation_key_material()
+    k = oracle_keys(pid)
+    assert (bsk == k.bsk).all() and (ksk == k.ksk).all()
+
+
+@pytest.mark.parametrize("pid", ALL_SETS)
 def test_encrypt_decrypt_matches_oracle(hb, oracle, oracle_keys, pid):
-    p = hb.Parameters.preset(pid)
+    p = hb_params_of(hb, pid)
     sk = hb.SecretKeyPack(p, 0)
     bits = np.random.default_rng(pid).integers(0, 2, 64).astype(np.uint8)
     c = sk.encrypt(bits, index0=100)
@@ -36,7 +46,7 @@ def test_encrypt_decrypt_matches_oracle(hb, oracle, oracle_keys, pid):
     mo, noiseo = oracle.decrypt(k.p, k.lwe_sk, c)
     assert (m == bits).all() and (mo == bits).all() and (noise == noiseo).all()
     g = np.load(GOLDEN)
-    name = oracle.PRESET_NAMES[pid]
+    name = oracle.SET_NAMES[pid]
     assert (sk.encrypt([0, 0, 1, 1], 0) == g[f"{name}/c0"]).all()
 
 
@@ -46,15 +56,27 @@ def test_parameter_validation(hb):
     raw = HbParams()
     assert lib().hb_params_preset(1, ctypes.byref(raw)) == 0
     assert lib().hb_params_validate(ctypes.byref(raw)) == 0
-    bad = [("ring_dim", 1000), ("lwe_dim", 300), ("br_len", 7), ("br_bits", 0), ("field_id", 5),
-           ("ring_dim", 8192)]
+    # n only needs next_pow2(n) <= N (n = 300 switches keys in two chunks of 512 words)
+    bad = [("ring_dim", 1000), ("lwe_dim", 2000), ("lwe_dim", 0), ("br_len", 7), ("br_bits", 0),
+           ("field_id", 5), ("ring_dim", 8192), ("lwe_ternary", 1), ("lwe_ternary", 2)]
     for field, value in bad:
         r = HbParams()
         lib().hb_params_preset(1, ctypes.byref(r))
         setattr(r, field, value)
         assert lib().hb_params_validate(ctypes.byref(r)) == -1, field
+    r = HbParams()
+    lib().hb_params_preset(1, ctypes.byref(r))
+    r.lwe_dim = 300
+    assert lib().hb_params_validate(ctypes.byref(r)) == 0
+    # ternary LWE keys: DefaultFieldU32 only (ternary.rs:80 marks the other fields incompatible)
+    r = HbParams()
+    lib().hb_params_preset(4, ctypes.byref(r))
+    r.lwe_ternary = 1
+    assert lib().hb_params_validate(ctypes.byref(r)) == 0
     with pytest.raises(HbError):
         hb.Parameters(bad_params())
+    with pytest.raises(HbError):
+        hb.Parameters.preset(0).with_ternary_lwe_key()
     assert lib().hb_params_preset(9, ctypes.byref(raw)) == -1
 
 

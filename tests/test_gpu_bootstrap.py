@@ -5,6 +5,7 @@ import os
 import numpy as np
 import pytest
 
+from conftest import ALL_SETS, hb_params_of
 from gpu_util import empty_dev, from_dev, to_dev
 
 pytestmark = pytest.mark.gpu
@@ -31,7 +32,7 @@ _EV = {}
 def evaluator(hb, ctx):
     def get(pid):
         if pid not in _EV:
-            sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(pid), 0)
+            sk = hb.KeyGen.generate_secret_key(hb_params_of(hb, pid), 0)
             _EV[pid] = (sk, hb.Evaluator(sk, ctx))
         return _EV[pid]
     yield get
@@ -40,9 +41,9 @@ def evaluator(hb, ctx):
     _EV.clear()
 
 
-@pytest.mark.parametrize("pid", [0, 1, 2])
+@pytest.mark.parametrize("pid", ALL_SETS)
 def test_nand_golden(oracle, golden, evaluator, pid):
-    name = oracle.PRESET_NAMES[pid]
+    name = oracle.SET_NAMES[pid]
     sk, ev = evaluator(pid)
     out = ev.nand(golden[f"{name}/c0"], golden[f"{name}/c1"])
     assert (out == golden[f"{name}/nand"]).all()
@@ -71,7 +72,8 @@ def test_bootstrap_custom_lut(oracle, golden, evaluator):
     assert (out == golden[f"{name}/bootstrap_lut"]).all()
 
 
-@pytest.mark.parametrize("pid,count", [(0, 45), (1, 9)])
+@pytest.mark.parametrize("pid,count", [(0, 45), (1, 9), (3, 7), (4, 31), (100, 13), (101, 6),
+                                       (102, 19)])
 def test_random_batch_vs_oracle_and_plain(hb, oracle, oracle_keys, evaluator, ctx, pid, count):
     """Batched launch (partial last CTA) == oracle == one-gate-per-launch form."""
     from hasteboots_b200._lib import check, lib
@@ -101,3 +103,22 @@ def test_device_tensors_large_batch(hb, evaluator, ctx):
     m, noise = sk.decrypt_with_noise(out)
     assert (m == 1 - (bits[0] & bits[1])).all()
     assert (noise < sk.params.modulus // 16).all()
+
+
+@pytest.mark.parametrize("pid", [3, 4, 100])
+def test_default_field_gates_vs_oracle(hb, oracle, oracle_keys, evaluator, pid):
+    """Every gate kind on the DefaultFieldU32 sets: one key-switching chunk (n = N), two chunks
+    (n = 512) and the ternary-LWE-key blind rotation, bit-exact against the oracle."""
+    sk, ev = evaluator(pid)
+    k = oracle_keys(pid)
+    bits = np.random.default_rng(300 + pid).integers(0, 2, (3, 6)).astype(np.uint8)
+    c = [sk.encrypt(bits[i], 5000 + 100 * i) for i in range(3)]
+    for g in ("and", "or", "nor", "xor", "xnor", "majority", "mux", "not"):
+        if g == "not":
+            out, ref = ev.not_(c[0]), oracle.gate(k, g, c[0])
+        elif g in ("majority", "mux"):
+            out, ref = getattr(ev, g)(*c), oracle.gate(k, g, *c)
+        else:
+            out = getattr(ev, g + "_" if g in ("and", "or") else g)(c[0], c[1])
+            ref = oracle.gate(k, g, c[0], c[1])
+        assert (out == ref).all(), g

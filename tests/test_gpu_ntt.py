@@ -10,7 +10,7 @@ from gpu_util import empty_dev, from_dev, ptr, to_dev
 
 pytestmark = pytest.mark.gpu
 
-CASES = [(1, 10), (1, 11), (0, 10), (0, 11)]
+CASES = [(1, 10), (1, 11), (0, 10), (0, 11), (2, 10), (2, 11)]
 
 
 def rand(oracle, field, shape, seed):
@@ -46,7 +46,7 @@ def _pointwise(a, b, q):
     return np.array([(int(u) * int(v)) % q for u, v in zip(a, b)], dtype=a.dtype)
 
 
-@pytest.mark.parametrize("field,log_n", [(1, 10), (0, 10), (1, 11)])
+@pytest.mark.parametrize("field,log_n", [(1, 10), (0, 10), (1, 11), (2, 10)])
 def test_ntt_forward_inverse_product(hb, oracle, ctx, field, log_n):
     from hasteboots_b200._lib import check, lib
     n = 1 << log_n
@@ -65,7 +65,8 @@ def test_ntt_forward_inverse_product(hb, oracle, ctx, field, log_n):
 
 
 @pytest.mark.parametrize("field,log_n,bits,length", [(1, 10, 5, 13), (1, 11, 5, 13),
-                                                     (1, 10, 8, 8), (0, 10, 8, 4), (0, 11, 5, 7)])
+                                                     (1, 10, 8, 8), (0, 10, 8, 4), (0, 11, 5, 7),
+                                                     (2, 10, 3, 9), (2, 10, 1, 27), (2, 11, 7, 4)])
 def test_external_product(hb, oracle, ctx, field, log_n, bits, length):
     from hasteboots_b200._lib import check, lib
     n = 1 << log_n

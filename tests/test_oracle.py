@@ -9,7 +9,7 @@ import pytest
 from conftest import rng
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_seed0.npz")
-FIELDS = [0, 1]
+FIELDS = [0, 1, 2]
 
 
 def rand_poly(oracle, field, n, seed):
@@ -53,7 +53,8 @@ def test_ntt_roundtrip_and_schoolbook(oracle, field, log_n):
                 oracle.negacyclic_mul(field, log_n, x, y, schoolbook=True)).all()
 
 
-@pytest.mark.parametrize("field,bits,length", [(1, 5, 13), (1, 8, 8), (0, 8, 4), (0, 5, 7)])
+@pytest.mark.parametrize("field,bits,length", [(1, 5, 13), (1, 8, 8), (0, 8, 4), (0, 5, 7),
+                                               (2, 3, 9), (2, 7, 4), (2, 1, 27)])
 def test_external_product_vs_plaintext(oracle, field, bits, length):
     # lattice/tests/lattice_test.rs:352-406: RGSW(m) x RLWE(p) decrypts to m*p. With a noiseless
     # "RGSW" of message 1 under key 0 (c_m rows = (0, B^j), c_neg_s_m rows = (B^j, 0)) the external
@@ -92,7 +93,7 @@ def test_keygen_deterministic_and_truth_tables(oracle, oracle_keys):
 def test_golden_fixtures_reproduce(oracle, oracle_keys):
     import hashlib
     g = np.load(GOLDEN)
-    for pid, name in oracle.PRESET_NAMES.items():
+    for pid, name in oracle.SET_NAMES.items():
         k = oracle_keys(pid)
         assert hashlib.sha256(k.bsk.tobytes()).hexdigest() == str(g[f"{name}/sha_bsk"])
         assert hashlib.sha256(k.ksk.tobytes()).hexdigest() == str(g[f"{name}/sha_ksk"])
@@ -102,3 +103,46 @@ def test_golden_fixtures_reproduce(oracle, oracle_keys):
         m, noise = oracle.decrypt(k.p, k.lwe_sk, g[f"{name}/nand"])
         assert (m == [1, 1, 1, 0]).all()
         assert (noise < oracle.MODULUS[k.p.field_id] // 16).all()
+
+
+@pytest.mark.parametrize("set_id", [3, 4, 100])
+def test_default_field_sets_truth_tables(oracle, oracle_keys, set_id):
+    # DEFAULT_TERNARY_128_BITS (n = N: one key-switching chunk), CUSTOM_TERNARY_128_BITS (n = 512:
+    # two chunks of 512) and the ternary-LWE-key blind rotation on the CUSTOM set.
+    k = oracle_keys(set_id)
+    p = k.p
+    if set_id == 100:
+        assert set(np.unique(k.lwe_sk)) == {0, 1, oracle.MODULUS[2] - 1}
+    else:
+        assert set(np.unique(k.lwe_sk)) <= {0, 1} and set(np.unique(k.ring_sk)) <= {0, 1}
+    bits = np.array([0, 0, 1, 1], np.uint8), np.array([0, 1, 0, 1], np.uint8)
+    c0 = oracle.encrypt(p, k.lwe_sk, 9, 0, bits[0])
+    c1 = oracle.encrypt(p, k.lwe_sk, 9, 4, bits[1])
+    for g, f in (("nand", lambda a, b: 1 - (a & b)), ("xor", lambda a, b: a ^ b)):
+        m, noise = oracle.decrypt(p, k.lwe_sk, oracle.gate(k, g, c0, c1))
+        assert (m == f(*bits)).all(), g
+        assert (noise < oracle.MODULUS[2] // 16).all(), g
+
+
+def test_cbd_error_polynomials(oracle):
+    # sigma exactly 3.2 selects sample_cbd_field_vec for RLWE error polynomials
+    # (algebra/src/random.rs:91-92); in a release build its a < b branch yields b - a for a
+    # 32-bit field, so every error coefficient lies in [0, 13].
+    p = oracle.preset(4)
+    p.ks_noise_std = 3.2
+    k = oracle.keygen(p, 2)
+    M, L = 512, p.ks_len
+    s = np.zeros(M, np.uint32)
+    s[:p.lwe_dim] = k.lwe_sk
+    q = oracle.MODULUS[2]
+    ksk = k.ksk.reshape(2, L, 2, M)
+    errs = []
+    for c in range(2):
+        z = k.ring_sk[c * M:(c + 1) * M].astype(np.uint64)
+        for j in range(L):
+            a_s = oracle.negacyclic_mul(2, 9, ksk[c, j, 0], s).astype(np.uint64)
+            zb = (z * pow(2, 7 * j, q)) % q
+            e = (ksk[c, j, 1].astype(np.uint64) + 2 * q - a_s - zb) % q
+            errs.append(e)
+    e = np.concatenate(errs)
+    assert e.max() <= 13 and e.min() == 0 and np.count_nonzero(e) > len(e) // 2
