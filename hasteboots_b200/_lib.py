@@ -32,6 +32,7 @@ EXPORTS = [
     "hb_batch_info", "hb_serve_start", "hb_serve_submit", "hb_serve_poll", "hb_serve_next_done",
     "hb_serve_fetch", "hb_serve_stats", "hb_serve_stop", "hb_gate_mux_device_noalloc",
     "hb_probe_modmul", "hb_ctx_launches", "hb_ctx_set_wait_limit", "hb_ctx_test_withhold_keys",
+    "hb_keys_generate", "hb_encrypt_device", "hb_keys_device_words", "hb_keys_download",
 ]
 
 
@@ -144,6 +145,10 @@ def lib():
         "hb_ctx_launches": (u64, [vp]),
         "hb_ctx_set_wait_limit": (i32, [vp, ctypes.c_longlong]),
         "hb_ctx_test_withhold_keys": (i32, [vp, i32]),
+        "hb_keys_generate": (i32, [vp, P, u64, vp, vp, pp]),
+        "hb_encrypt_device": (i32, [vp, P, vp, u64, u64, vp, sz, vp]),
+        "hb_keys_device_words": (i32, [vp, ctypes.POINTER(sz), ctypes.POINTER(sz)]),
+        "hb_keys_download": (i32, [vp, vp, vp, sz, vp, sz]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

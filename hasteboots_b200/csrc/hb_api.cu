@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/hb_gpu.h"
+#include "hb_keygen.cuh"
 #include "hb_kernels.cuh"
 #include "hb_runtime.h"
 
@@ -735,6 +736,31 @@ int hb_keys_params(const hb_keys *keys, hb_params *out) {
   return HB_OK;
 }
 
+int hb_keys_device_words(const hb_keys *keys, size_t *bsk_words, size_t *ksk_words) {
+  if (!keys) return HB_ERR_INVALID;
+  size_t nb = 0;
+  hb_params_sizes(&keys->p, nullptr, nullptr, &nb, nullptr, nullptr);
+  if (bsk_words) *bsk_words = nb;
+  if (ksk_words) *ksk_words = ksk_device_words(keys->p);
+  return HB_OK;
+}
+
+int hb_keys_download(hb_ctx *ctx, const hb_keys *keys, void *bsk, size_t bsk_words, void *ksk,
+                     size_t ksk_words) {
+  if (!ctx || !keys || !bsk || !ksk) return HB_ERR_INVALID;
+  size_t nb = 0, nk = 0;
+  hb_keys_device_words(keys, &nb, &nk);
+  if (bsk_words != nb || ksk_words != nk)
+    return fail(ctx, HB_ERR_INVALID, "key buffers of %zu / %zu words, the keys hold %zu / %zu", bsk_words,
+                ksk_words, nb, nk);
+  cudaSetDevice(ctx->device);
+  const size_t ws = word_size(keys->p);
+  cudaError_t e = cudaMemcpyAsync(bsk, keys->bsk, nb * ws, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ksk, keys->ksk, nk * ws, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? HB_OK : cuda_fail(ctx, e, "key download");
+}
+
 int hb_gate_device(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1,
                    const void *c2, void *out, size_t count) {
   if (!ctx || !keys) return HB_ERR_INVALID;
@@ -975,6 +1001,160 @@ int hb_ctx_test_withhold_keys(hb_ctx *ctx, int on) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Key generation and encryption on the device
+// ------------------------------------------------------------------------------------------
+
+namespace {
+
+template <class F, int LOGN, int T>
+int launch_keygen(hb_ctx *ctx, hb::KeygenParams<typename F::W> &prm) {
+  using W = typename F::W;
+  constexpr int N = 1 << LOGN;
+  DevTables *tb;
+  int rc = tables(ctx, F::FIELD_ID, LOGN, &tb, hb::GroupNtt<F, LOGN, T>::LOGV);
+  if (rc) return rc;
+  prm.tw = (const W *)tb->tw;
+  prm.itw = (const W *)tb->itw;
+  prm.scale = (W)tb->key_scale;
+  auto kern = hb::keygen_rows_kernel<F, LOGN, T>;
+  const size_t smem = sizeof(W) * (2 * N + 2 * 2 * N);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((prm.rows + 1) / 2, (size_t)ctx->sms * 4));
+  kern<<<grid, 2 * T, smem, ctx->stream>>>(prm);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? HB_OK : cuda_fail(ctx, e, "keygen launch");
+}
+
+// BSK and KSK rows of p on the device into keys->bsk / keys->ksk (slot layout of keys'
+// threads_per_gate), from the secret keys lwe_sk / ring_sk (host words).
+template <class F>
+int generate_keys(hb_ctx *ctx, const hb_params &p, uint64_t seed, const void *lwe_sk,
+                  const void *ring_sk, hb_keys *k) {
+  using W = typename F::W;
+  const uint32_t N = p.ring_dim, n = p.lwe_dim, M = ks_dim(p), stride = N / M;
+  if (N != 1024) return fail(ctx, HB_ERR_UNSUPPORTED, "device key generation is compiled for N = 1024");
+  // device copies: LWE key, ring key, and both multiplier keys (ring key z for the BSK rows, the
+  // LWE key padded to n' words and spread to N for the KSK rows) before their transforms
+  std::vector<W> host(2 * (size_t)N, 0);
+  std::memcpy(host.data(), ring_sk, sizeof(W) * N);
+  for (uint32_t u = 0; u < n; ++u) host[N + (size_t)u * stride] = ((const W *)lwe_sk)[u];
+  void *d_tmp = nullptr;
+  int rc = dev_alloc(ctx, sizeof(W) * (6 * (size_t)N + n), &d_tmp);
+  if (rc) return rc;
+  W *d_raw = (W *)d_tmp, *d_keys = d_raw + 2 * N, *d_ring = d_keys + 2 * N, *d_lwe = d_ring + N;
+  cudaError_t e = cudaMemcpyAsync(d_raw, host.data(), sizeof(W) * 2 * N, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_ring, ring_sk, sizeof(W) * N, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_lwe, lwe_sk, sizeof(W) * n, cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) rc = cuda_fail(ctx, e, "key generation upload");
+  const int T = k->threads_per_gate;
+  if (!rc) rc = prepare_field(ctx, p.field_id, 10, T, d_raw, d_keys, 2);
+  hb::KeygenParams<W> prm{};
+  prm.lwe_sk = d_lwe;
+  prm.ring_sk = d_ring;
+  prm.seed = seed;
+  prm.n = n;
+  prm.len = p.br_len;
+  prm.bits = p.br_bits;
+  prm.pairs = p.lwe_ternary ? 2 : 1;
+  prm.ks_n = M;
+  prm.ks_len = p.ks_len;
+  W pw = 1;
+  const W bks = (W)(1ULL << p.ks_bits);
+  for (uint32_t j = 0; j < p.ks_len && j < 64; ++j) {
+    prm.ks_pow[j] = F::to_mont(pw);
+    pw = hb::host_mulmod<F>(pw, bks);
+  }
+  auto launch = [&](void) -> int {
+    if (T == 64) return launch_keygen<F, 10, 64>(ctx, prm);
+    if (T == 128) return launch_keygen<F, 10, 128>(ctx, prm);
+    return fail(ctx, HB_ERR_UNSUPPORTED, "no key generation kernel for %d threads per gate", T);
+  };
+  if (!rc) {  // RGSW rows under the ring key
+    prm.out = (W *)k->bsk;
+    prm.key = d_keys;
+    prm.sigma = p.ring_noise_std;
+    prm.rows = n * prm.pairs * 2 * p.br_len;
+    prm.ksk = 0;
+    rc = launch();
+  }
+  if (!rc) {  // key-switching rows under the padded LWE key
+    prm.out = (W *)k->ksk;
+    prm.key = d_keys + N;
+    prm.sigma = p.ks_noise_std;
+    prm.rows = (N / M) * p.ks_len;
+    prm.ksk = 1;
+    rc = launch();
+  }
+  e = cudaStreamSynchronize(ctx->stream);
+  dev_free(ctx, d_tmp);
+  if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "key generation");
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int hb_keys_generate(hb_ctx *ctx, const hb_params *p, uint64_t seed, void *lwe_sk,
+                                void *ring_sk, hb_keys **out) {
+  if (!ctx || !out || !lwe_sk || !ring_sk) return HB_ERR_INVALID;
+  *out = nullptr;
+  if (hb_params_validate(p) != HB_OK) return fail(ctx, HB_ERR_INVALID, "invalid parameter set");
+  if (p->ks_len > 64) return fail(ctx, HB_ERR_UNSUPPORTED, "more than 64 key-switching digits");
+  // the secret keys are drawn on the host (n + N words): KeyGen::generate_secret_key
+  int rc = hb_keygen(p, seed, lwe_sk, ring_sk, nullptr, nullptr, 1);
+  if (rc) return fail(ctx, rc, "secret key generation");
+  cudaSetDevice(ctx->device);
+  size_t nb = 0;
+  hb_params_sizes(p, nullptr, nullptr, &nb, nullptr, nullptr);
+  const size_t nkd = ksk_device_words(*p), ws = word_size(*p);
+  hb_keys *k = new hb_keys();
+  k->p = *p;
+  k->threads_per_gate = default_threads_per_gate(p->field_id);
+  rc = dev_alloc(ctx, nb * ws, &k->bsk);
+  if (!rc) rc = dev_alloc(ctx, nkd * ws, &k->ksk);
+  if (!rc) {
+    if (p->field_id == HB_FIELD_GOLDILOCKS)
+      rc = generate_keys<Goldilocks>(ctx, *p, seed, lwe_sk, ring_sk, k);
+    else if (p->field_id == HB_FIELD_BABYBEAR)
+      rc = generate_keys<BabyBear>(ctx, *p, seed, lwe_sk, ring_sk, k);
+    else
+      rc = generate_keys<DefaultFieldU32>(ctx, *p, seed, lwe_sk, ring_sk, k);
+  }
+  if (rc) {
+    dev_free(ctx, k->bsk);
+    dev_free(ctx, k->ksk);
+    delete k;
+    return rc;
+  }
+  k->bytes = (nb + nkd) * ws;
+  k->gates_per_cta = default_gates_per_cta(p->field_id);
+  const std::vector<int> cand = variants(*p, k->threads_per_gate);
+  if (cand.size() && std::find(cand.begin(), cand.end(), k->gates_per_cta) == cand.end())
+    k->gates_per_cta = cand.back();
+  *out = k;
+  return HB_OK;
+}
+
+extern "C" int hb_encrypt_device(hb_ctx *ctx, const hb_params *p, const void *d_lwe_sk, uint64_t seed,
+                                 uint64_t index0, const uint8_t *d_bits, size_t count, void *d_out) {
+  if (!ctx || !d_lwe_sk || (count && (!d_bits || !d_out))) return HB_ERR_INVALID;
+  if (hb_params_validate(p) != HB_OK) return fail(ctx, HB_ERR_INVALID, "invalid parameter set");
+  if (count == 0) return HB_OK;
+  cudaSetDevice(ctx->device);
+  const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((count + 7) / 8, (size_t)ctx->sms * 16));
+  if (p->field_id == HB_FIELD_GOLDILOCKS)
+    hb::lwe_encrypt_kernel<Goldilocks><<<grid, 256, 0, ctx->stream>>>(
+        (const uint64_t *)d_lwe_sk, d_bits, (uint64_t *)d_out, count, p->lwe_dim, seed, index0, p->lwe_noise_std);
+  else if (p->field_id == HB_FIELD_BABYBEAR)
+    hb::lwe_encrypt_kernel<BabyBear><<<grid, 256, 0, ctx->stream>>>(
+        (const uint32_t *)d_lwe_sk, d_bits, (uint32_t *)d_out, count, p->lwe_dim, seed, index0, p->lwe_noise_std);
+  else
+    hb::lwe_encrypt_kernel<DefaultFieldU32><<<grid, 256, 0, ctx->stream>>>(
+        (const uint32_t *)d_lwe_sk, d_bits, (uint32_t *)d_out, count, p->lwe_dim, seed, index0, p->lwe_noise_std);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? HB_OK : cuda_fail(ctx, e, "encrypt launch");
+}
 
 // ------------------------------------------------------------------------------------------
 // Allocation-free MUX (hb_gate_mux_device_noalloc)

@@ -1,16 +1,11 @@
 // hb_client.cpp -- host-side parameters, key generation, encryption and decryption
 // (the tfhe crate's KeyGen / Encryptor / Decryptor and Evaluator::new key material).
 //
-// Seeded key convention: every random value is drawn from a counter PRG
-//   rand(seed, stream, ctr) = mix(mix(seed + g) ^ mix(stream ^ c) + ctr * g)
-// (mix = splitmix64 finaliser), so key generation parallelises over polynomials and is identical on
-// every host. Streams: (tag, i, part, j, which) packed into 64 bits. Distributions follow the
-// reference: binary or ternary {0,0,1,-1}[r&3] LWE and ring keys (algebra/src/utils/sample.rs:6-51),
-// uniform field elements, and the discrete Gaussian of FieldDiscreteGaussianSampler
-// (algebra/src/random.rs:156-171: N(0, sigma), reject |x| >= 6 sigma, round half away from zero,
-// negative r -> Q - |r|) with normal deviates from the Marsaglia polar method and a logarithm built
-// from IEEE-exact operations; error polynomials with sigma exactly 3.2 come from the centered
-// binomial sampler instead (algebra/src/random.rs:91-92, algebra/src/utils/sample.rs:54-75).
+// Seeded key convention: every random value is drawn from the counter PRG of hb_sample.cuh, so key
+// generation parallelises over polynomials and is identical on every host and on the device
+// (hb_keys_generate). Distributions follow the reference: binary or ternary {0,0,1,-1}[r&3] LWE and
+// ring keys (algebra/src/utils/sample.rs:6-51), uniform field elements, the discrete Gaussian and,
+// for error polynomials with sigma exactly 3.2, the centered binomial sampler (hb_sample.cuh).
 
 #include <algorithm>
 #include <atomic>
@@ -21,6 +16,7 @@
 
 #include "../../include/hb_gpu.h"
 #include "hb_field.cuh"
+#include "hb_sample.cuh"
 
 namespace {
 
@@ -46,91 +42,17 @@ struct HostField {
   static W neg(W a) { return a == 0 ? 0 : (W)(F::P - a); }
 };
 
-// ---- PRG ----
-inline u64 mix(u64 z) {
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-  return z ^ (z >> 31);
-}
-inline u64 rnd(u64 seed, u64 stream, u64 ctr) {
-  const u64 key = mix(seed + 0x9E3779B97F4A7C15ULL) ^ mix(stream ^ 0xD1B54A32D192ED03ULL);
-  return mix(key + ctr * 0x9E3779B97F4A7C15ULL);
-}
-constexpr u64 kTagLweSk = 1, kTagRingSk = 2, kTagBsk = 3, kTagKsk = 4, kTagEnc = 5;
-inline u64 stream_of(u64 tag, u64 i, u64 part, u64 j, u64 which) {
-  return (tag << 56) | ((i & 0xFFFFFFFFULL) << 24) | ((part & 0xFF) << 16) | ((j & 0xFF) << 8) |
-         (which & 0xFF);
-}
-
-// ln(s), s in (0, 1]: s = m 2^e with m in [1/sqrt2, sqrt2), ln s = e ln2 + 2 atanh((m-1)/(m+1)),
-// atanh by its odd power series (24 terms; |y| <= 0.1716).
-double log_unit(double s) {
-  int e;
-  double m = std::frexp(s, &e);
-  if (m < 0.70710678118654752440) {
-    m = m * 2.0;
-    e = e - 1;
-  }
-  const double y = (m - 1.0) / (m + 1.0);
-  const double y2 = y * y;
-  double acc = 0.0;
-  double pw = y;
-  for (int k = 0; k < 24; ++k) {
-    acc = acc + pw / (double)(2 * k + 1);
-    pw = pw * y2;
-  }
-  return 2.0 * acc + (double)e * 0.693147180559945309417232121458;
-}
-
-inline double to_unit(u64 r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
-
-template <class F>
-typename F::W sample_gauss(u64 seed, u64 stream, u64 coeff, double sigma) {
-  const double bound = sigma * 6.0;
-  for (u64 attempt = 0;; ++attempt) {
-    const u64 ctr = (coeff << 20) | (attempt << 1);
-    const double u = 2.0 * to_unit(rnd(seed, stream, ctr)) - 1.0;
-    const double v = 2.0 * to_unit(rnd(seed, stream, ctr | 1)) - 1.0;
-    const double s = u * u + v * v;
-    if (!(s > 0.0 && s < 1.0)) continue;
-    const double z = u * std::sqrt(-2.0 * log_unit(s) / s);
-    const double val = sigma * z;
-    if (std::fabs(val) >= bound) continue;
-    const double r = std::round(val);
-    if (r < 0.0) return (typename F::W)((u64)F::P - (u64)(-r));
-    return (typename F::W)(u64)r;
-  }
-}
-
-template <class F>
-inline typename F::W sample_uniform(u64 seed, u64 stream, u64 k) {
-  return (typename F::W)(rnd(seed, stream, k) % (u64)F::P);
-}
-
-// sample_cbd_field_vec (algebra/src/utils/sample.rs:54-75) on the low six bytes of one PRG word:
-// popcounts a (bytes 0, 1 and 5 bits of byte 2) and b (bytes 3, 4 and 5 bits of byte 5). For a < b
-// the reference's `modulus - (a - b)` wraps its u32 subtraction (release builds), which leaves
-// Field::new of the wrapped word in the field's width: b - a for 32-bit fields,
-// P - (2^32 - (b - a)) for Goldilocks.
-template <class F>
-typename F::W sample_cbd(u64 seed, u64 stream, u64 k) {
-  using W = typename F::W;
-  const u64 r = rnd(seed, stream, k);
-  auto pc = [](u64 x) { return (uint32_t)__builtin_popcountll(x); };
-  const uint32_t a = pc(r & 0xFF) + pc((r >> 8) & 0xFF) + pc((r >> 16) & 0x1F);
-  const uint32_t b = pc((r >> 24) & 0xFF) + pc((r >> 32) & 0xFF) + pc((r >> 40) & 0x1F);
-  const uint32_t d = a - b;
-  if (a >= b) return (W)d;
-  const W v = (W)((W)F::P - (W)d);
-  return (W)((u64)v % (u64)F::P);
-}
-
-// One coefficient of an error polynomial (Polynomial::random_with_gaussian,
-// algebra/src/polynomial/univariate/native_polynomial.rs:232-246).
-template <class F>
-typename F::W error_coeff(u64 seed, u64 stream, u64 k, double sigma) {
-  return sigma == 3.2 ? sample_cbd<F>(seed, stream, k) : sample_gauss<F>(seed, stream, k, sigma);
-}
+// ---- samplers (hb_sample.cuh, shared with the device key generator) ----
+using hb::smp::error_coeff;
+using hb::smp::kTagBsk;
+using hb::smp::kTagEnc;
+using hb::smp::kTagKsk;
+using hb::smp::kTagLweSk;
+using hb::smp::kTagRingSk;
+using hb::smp::rnd;
+using hb::smp::sample_gauss;
+using hb::smp::sample_uniform;
+using hb::smp::stream_of;
 
 // Calls fn(F{}) with the field type of a field id (Goldilocks, BabyBear or DefaultFieldU32).
 template <class Fn>
@@ -342,8 +264,7 @@ void keygen_impl(const hb_params *p, u64 seed, typename F::W *lwe_sk, typename F
 
 template <class F>
 u64 encode_msg(u64 m) {
-  const double q = (double)(u64)F::P;
-  return (u64)std::round((double)m * (q / 4.0));  // fhe_core/src/plaintext.rs:64-75, t = 4
+  return hb::smp::encode_msg<F>(m);  // fhe_core/src/plaintext.rs:64-75, t = 4
 }
 template <class F>
 u64 decode_msg(u64 c) {

@@ -206,15 +206,40 @@ class Context:
 class DeviceKeys:
     """Device-resident BSK/KSK (hb_keys)."""
 
-    def __init__(self, ctx: Context, params: Parameters, bsk, ksk):
-        h = ctypes.c_void_p()
-        bsk = np.ascontiguousarray(bsk, params.dtype)
-        ksk = np.ascontiguousarray(ksk, params.dtype)
-        check(lib().hb_keys_upload(ctx.handle, ctypes.byref(params.raw), _ptr(bsk), _ptr(ksk),
-                                   ctypes.byref(h)), "hb_keys_upload", ctx.handle)
+    def __init__(self, ctx: Context, params: Parameters, bsk=None, ksk=None, handle=None):
+        if handle is None:
+            h = ctypes.c_void_p()
+            bsk = np.ascontiguousarray(bsk, params.dtype)
+            ksk = np.ascontiguousarray(ksk, params.dtype)
+            check(lib().hb_keys_upload(ctx.handle, ctypes.byref(params.raw), _ptr(bsk), _ptr(ksk),
+                                       ctypes.byref(h)), "hb_keys_upload", ctx.handle)
+            handle = h
         self.ctx = ctx
         self.params = params
-        self.handle = h
+        self.handle = handle
+
+    @classmethod
+    def generate(cls, ctx: Context, params: Parameters, seed=0):
+        """Evaluator::new's key material generated on the device (hb_keys_generate): the same
+        words as the host generator followed by an upload. Returns (keys, lwe_sk, ring_sk)."""
+        s = params.sizes()
+        lwe = np.zeros(s["lwe_sk"], params.dtype)
+        ring = np.zeros(s["ring_sk"], params.dtype)
+        h = ctypes.c_void_p()
+        check(lib().hb_keys_generate(ctx.handle, ctypes.byref(params.raw), seed, _ptr(lwe), _ptr(ring),
+                                     ctypes.byref(h)), "hb_keys_generate", ctx.handle)
+        return cls(ctx, params, handle=h), lwe, ring
+
+    def download(self):
+        """The device words of the keys (transformed, scaled, kernel slot layout): (bsk, ksk)."""
+        nb, nk = ctypes.c_size_t(), ctypes.c_size_t()
+        check(lib().hb_keys_device_words(self.handle, ctypes.byref(nb), ctypes.byref(nk)),
+              "hb_keys_device_words")
+        bsk = np.zeros(nb.value, self.params.dtype)
+        ksk = np.zeros(nk.value, self.params.dtype)
+        check(lib().hb_keys_download(self.ctx.handle, self.handle, _ptr(bsk), nb.value, _ptr(ksk),
+                                     nk.value), "hb_keys_download", self.ctx.handle)
+        return bsk, ksk
 
     def free(self):
         if self.handle and self.ctx.handle:
@@ -225,10 +250,17 @@ class DeviceKeys:
 class Evaluator:
     """tfhe::Evaluator (tfhe/src/bfhe/evaluate.rs:65-262) on one B200."""
 
-    def __init__(self, sk: SecretKeyPack, ctx: Context = None, keys=None):
+    def __init__(self, sk: SecretKeyPack, ctx: Context = None, keys=None, device_keygen=True):
+        """Keys generated on the device by default (hb_keys_generate); device_keygen=False runs the
+        host generator and uploads its coefficient-domain keys. Both give the same device words."""
         self.params = sk.params
         self.ctx = ctx or Context()
-        if keys is None:
+        if keys is None and device_keygen:
+            keys, lwe, ring = DeviceKeys.generate(self.ctx, self.params, sk.seed)
+            if not ((lwe == sk.lwe_secret_key).all() and (ring == sk.ring_secret_key).all()):
+                keys.free()
+                raise ValueError("secret keys differ from the key pack's")
+        elif keys is None:
             bsk, ksk = sk.evaluation_key_material()
             keys = DeviceKeys(self.ctx, self.params, bsk, ksk)
         self.keys = keys

@@ -112,6 +112,10 @@ int hb_keygen(const hb_params *p, uint64_t seed, void *lwe_sk, void *ring_sk, vo
  * uses sample index index0 + i. */
 int hb_encrypt(const hb_params *p, const void *lwe_sk, uint64_t seed, uint64_t index0,
                const uint8_t *bits, size_t count, void *lwe_out);
+/* hb_encrypt on the device: d_lwe_sk (n words), d_bits (count bytes) and d_out (count ciphertexts)
+ * are device buffers; enqueued on the context stream. Same ciphertexts as hb_encrypt. */
+int hb_encrypt_device(hb_ctx *ctx, const hb_params *p, const void *d_lwe_sk, uint64_t seed,
+                      uint64_t index0, const uint8_t *d_bits, size_t count, void *d_out);
 /* Decryptor::decrypt / SecretKeyPack::decrypt_with_noise (fhe_core/src/secret_key.rs:151-188);
  * noise_out may be NULL. */
 int hb_decrypt(const hb_params *p, const void *lwe_sk, const void *lwe, size_t count,
@@ -133,8 +137,20 @@ size_t hb_ctx_hbm_in_use(const hb_ctx *ctx);
 
 /* Upload coefficient-domain BSK/KSK; transforms and lays them out on the device. */
 int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void *ksk, hb_keys **out);
+/* KeyGen::generate_secret_key + Evaluator::new (tfhe/src/key_gen.rs:12,
+ * tfhe/src/bfhe/evaluate.rs:26-39, fhe_core/src/blind_rotation/rlwe/binary.rs:207-239,
+ * ternary.rs:123-183, fhe_core/src/key_switch/rlwe.rs:37-112) with the key material generated on
+ * the device: the secret keys (n and N words) are written to lwe_sk / ring_sk, and the evaluation
+ * keys come out identical, word for word, to hb_keygen followed by hb_keys_upload. */
+int hb_keys_generate(hb_ctx *ctx, const hb_params *p, uint64_t seed, void *lwe_sk, void *ring_sk,
+                     hb_keys **out);
 void hb_keys_free(hb_ctx *ctx, hb_keys *keys);
 int hb_keys_params(const hb_keys *keys, hb_params *out);
+/* No counterpart in the reference: the words of the device-resident keys (transformed, scaled,
+ * in the bootstrap kernel's slot layout), for inspection and for tests of key generation. */
+int hb_keys_device_words(const hb_keys *keys, size_t *bsk_words, size_t *ksk_words);
+int hb_keys_download(hb_ctx *ctx, const hb_keys *keys, void *bsk, size_t bsk_words, void *ksk,
+                     size_t ksk_words);
 
 /* ---- gate bootstrapping --------------------------------------------------------------------- */
 
