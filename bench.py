@@ -431,7 +431,9 @@ def workload_serve(args):
 
 
 def workload_single(args):
-    """One BabyBear NAND gate, one launch (config 1): latency of the plain form."""
+    """One BabyBear NAND gate (config 1): latency of one hb_gate_device call (the latency form: one
+    CTA whose thread groups share the gate's digits), with the plain form (one kernel launch of a
+    single 64-thread group) beside it."""
     import torch
     from hasteboots_b200 import tfhe
     from hasteboots_b200._lib import check, lib
@@ -442,24 +444,33 @@ def workload_single(args):
     d0 = torch.from_numpy(c0.view(np.int32).copy()).cuda()
     d1 = torch.from_numpy(c1.view(np.int32).copy()).cuda()
     do = torch.zeros_like(d0)
+    dp = torch.zeros_like(d0)
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(ctx.stream_ptr())
-    one = lambda: check(lib().hb_gate_device_plain(ctx.handle, ev.keys.handle, 0, d0.data_ptr(), d1.data_ptr(),
-                                                   do.data_ptr(), 1), "plain", ctx.handle)
+    gate = lambda: check(lib().hb_gate_device(ctx.handle, ev.keys.handle, 0, d0.data_ptr(), d1.data_ptr(), None,
+                                              do.data_ptr(), 1), "gate", ctx.handle)
+    plain = lambda: check(lib().hb_gate_device_plain(ctx.handle, ev.keys.handle, 0, d0.data_ptr(), d1.data_ptr(),
+                                                     dp.data_ptr(), 1), "plain", ctx.handle)
     for _ in range(args.warmup):
-        one()
-    times = [_timed(stream, one, 1) for _ in range(args.steps)]
-    bit = sk.decrypt(do.cpu().numpy().view(np.uint32))[0]
+        gate()
+        plain()
+    times = [_timed(stream, gate, 1) for _ in range(args.steps)]
+    ptimes = [_timed(stream, plain, 1) for _ in range(args.steps)]
+    out = do.cpu().numpy().view(np.uint32)
+    bit = sk.decrypt(out)[0]
+    same = bool((out == dp.cpu().numpy().view(np.uint32)).all())
     line = {"metric": "single NAND bootstrap latency, BABYBEAR_BINARY_128_BITS", "value": float(np.median(times)),
             "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "dtype": "u32", "data": "synthetic (seed-0 keys)",
             "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
-            "config": {"workload": "1 NAND gate, one kernel launch (one 64-thread group)"},
-            "checks": {"nand(1,1)=0": bool(bit == 0)}}
+            "plain_form_ms": {"p50": float(np.percentile(ptimes, 50)), "p99": float(np.percentile(ptimes, 99))},
+            "config": {"workload": "1 NAND gate through hb_gate_device: one CTA of 8 thread groups sharing the "
+                                   "gate's digits; plain form: one launch of one 64-thread group"},
+            "checks": {"nand(1,1)=0": bool(bit == 0), "equals_plain_form": same}}
     print(json.dumps(line), flush=True)
     ev.keys.free()
     ctx.close()
-    return 0 if bit == 0 else 1
+    return 0 if (bit == 0 and same) else 1
 
 
 def main():

@@ -416,6 +416,24 @@ void boot_params(hb::BootParams<W> &prm, hb_ctx *ctx, const hb_keys *keys, const
   prm.withhold = ctx->withhold_keys;
 }
 
+// Launches of at most one gate per SM (G = 1 outside the plain form) run the latency form: one gate
+// per CTA, its digits spread over the CTA's thread groups (binary LWE keys, one key-switching chunk).
+template <class F, int LOGN, int T>
+int launch_dp(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream) {
+  using W = typename F::W;
+  constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T>();
+  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D>;
+  const size_t smem = hb::dp_smem_bytes<W, N, D>(prm.n);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
+  const unsigned grid = std::max(1u, std::min<unsigned>(prm.total_batches, (unsigned)ctx->sms));
+  kern<<<grid, D * T, smem, stream>>>(prm);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
+  ctx->launches += 1;
+  return HB_OK;
+}
+
 template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
 int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain) {
   using W = typename F::W;
@@ -450,6 +468,7 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
     prm.jobs = djobs;
     prm.njobs = (int)jobs.size();
     prm.total_batches = batches;
+    if constexpr (G == 1 && !TERN && !KSC) return launch_dp<F, LOGN, T>(ctx, prm, ctx->stream);
     kern<<<grid, block, smem, ctx->stream>>>(prm);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
@@ -543,6 +562,7 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
   prm.jobs = djobs;
   prm.njobs = njobs;
   prm.total_batches = batches;
+  if constexpr (G == 1 && !TERN && !KSC) return launch_dp<F, LOGN, T>(ctx, prm, stream);
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);

@@ -10,6 +10,8 @@
 //                           with accumulators in shared memory, key switching and sample extraction,
 //                           G gates per CTA sharing every bootstrapping-key chunk, which the TMA unit
 //                           streams into a ring of shared-memory stages
+//  * bootstrap_dp_kernel    the same bootstrap for launches of at most one gate per SM: one gate
+//                           per CTA with its gadget digits spread over the CTA's thread groups
 //  * modmul_probe_kernel    field-multiply throughput (the roofline denominator)
 #pragma once
 
@@ -766,6 +768,209 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
 aborted:
   __syncthreads();
   if (*s_abort) pipe.drain();
+}
+
+// ------------------------------------------------------------------------------------------
+// Latency form: one gate per CTA, its gadget digits spread over D thread groups
+// ------------------------------------------------------------------------------------------
+
+// Groups per CTA of bootstrap_dp_kernel: as many T-thread groups as 512 threads hold (the 64-bit
+// transforms keep about 128 registers a thread, so 4 groups of 128 or of 64).
+template <class W, int T>
+__host__ __device__ constexpr int dp_groups() {
+  return sizeof(W) == 8 ? 4 : 512 / T;
+}
+
+// Shared memory of bootstrap_dp_kernel: twiddles (2N words), the accumulator (2N), the
+// decomposition sources E.a and E.b (2N), per group two exchange buffers (2N) that also carry the
+// group's partial sums, and the modulus-switched input.
+template <class W, int N, int D>
+__host__ __device__ constexpr size_t dp_smem_bytes(uint32_t n) {
+  return sizeof(W) * (size_t)(6 + 2 * D) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
+}
+
+// The same bootstrap as bootstrap_kernel (binary LWE key, one key-switching chunk) with the
+// latency of one gate cut instead of the cost of many: per blind-rotation step the 2l digit
+// polynomials of E = ACC (X^r - 1) go to D groups (digit d to group d mod D), each transforms its
+// digits and multiply-accumulates them with their key rows read straight from global memory
+// (no staging, no waits), the groups' partial sums meet in shared memory, and groups 0 and 1
+// inverse-transform the a and b sums and add them to the accumulator. The key switch spreads its
+// l_ks digits the same way. Used for launches of at most one gate per SM.
+template <class F, int LOGN, int T, int D>
+__global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams<typename F::W> p) {
+  using W = typename F::W;
+  using NT = GroupNtt<F, LOGN, T>;
+  constexpr int N = 1 << LOGN, V = NT::V, NT_ALL = D * T;
+  static_assert(D >= 2, "groups 0 and 1 transform the a and b sums");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  W *s_tw = reinterpret_cast<W *>(smem_raw);
+  W *s_itw = s_tw + N;
+  W *acc_a = s_itw + N;
+  W *acc_b = acc_a + N;
+  W *s_e = acc_b + N;  // E.a then E.b (the key switch: -acc.a), natural order
+  W *s_x = s_e + 2 * N;
+  uint16_t *ms = reinterpret_cast<uint16_t *>(s_x + D * 2 * N);
+
+  const int tid = threadIdx.x, g = tid / T, t = tid % T;
+  for (int i = tid; i < N; i += NT_ALL) {
+    s_tw[i] = p.tw[i];
+    s_itw[i] = p.itw[i];
+  }
+  __syncthreads();
+  GroupSync<T> sync{1 + g};
+  W *xbuf = s_x + g * 2 * N;
+  int ping = 0;
+
+  const uint32_t n = p.n, L = p.len, two_n = 2 * N;
+  // products each group accumulates per phase (digits g, g + D, ...), for the lazy offsets
+  const uint32_t nd_br = 2 * L, nd_ks = p.ks_len;
+  const uint32_t my_br = (uint32_t)g < nd_br ? (nd_br - 1 - g) / D + 1 : 0;
+  const uint32_t my_ks = (uint32_t)g < nd_ks ? (nd_ks - 1 - g) / D + 1 : 0;
+  const W off_br = F::acc_offset(my_br);
+  const W off_ks = F::acc_offset(my_ks);
+
+  for (uint32_t gi = blockIdx.x; gi < p.total_batches; gi += gridDim.x) {
+    int jx = 0;
+    while (jx + 1 < p.njobs && p.jobs[jx + 1].first_batch <= gi) ++jx;
+    const GateJob &job = p.jobs[jx];
+    const uint32_t gate = gi - job.first_batch;  // one gate per batch
+    const size_t lwe_words = (size_t)n + 1;
+
+    // ---- input combine + modulus switch (as bootstrap_kernel) ----
+    {
+      const W *c0 = reinterpret_cast<const W *>(job.in0) + gate * lwe_words;
+      const W *c1 = job.in1 ? reinterpret_cast<const W *>(job.in1) + gate * lwe_words : nullptr;
+      const W *c2 = job.in2 ? reinterpret_cast<const W *>(job.in2) + gate * lwe_words : nullptr;
+      for (uint32_t k = tid; k <= n; k += NT_ALL) {
+        W c = small_mul<F>(c0[k], job.s0);
+        if (c1) c = F::canon(F::add(c, small_mul<F>(c1[k], job.s1)));
+        if (c2) c = F::canon(F::add(c, small_mul<F>(c2[k], job.s2)));
+        if (k == n) c = F::canon(F::add(c, (W)job.add_b));
+        ms[k] = (uint16_t)modswitch<F>(c, two_n);
+      }
+    }
+    __syncthreads();
+    // ---- ACC = (0, LUT * X^{-b}) (fhe_core/src/blind_rotation/rlwe/binary.rs:40-64) ----
+    {
+      const uint32_t bt = ms[n];
+      const int e = bt ? (int)(two_n - bt) : 0;
+      const W *lut = reinterpret_cast<const W *>(job.lut);
+      for (int k = tid; k < N; k += NT_ALL) {
+        int s = k - e;
+        bool neg = false;
+        if (s < 0) {
+          s += N;
+          neg = true;
+          if (s < 0) {
+            s += N;
+            neg = false;
+          }
+        }
+        W f = lut ? F::canon(lut[s]) : (W)((uint32_t)s < job.lut_mid ? job.lut_lo : job.lut_hi);
+        acc_a[k] = 0;
+        acc_b[k] = neg ? F::neg_ref(f) : f;
+      }
+    }
+    __syncthreads();
+
+    // ---- phases 0 .. n-1: blind-rotation steps; phase n: key switch ----
+    for (uint32_t ph = 0; ph <= n; ++ph) {
+      const bool ks = ph == n;
+      if (!ks) {
+        // E = ACC * (X^r - 1) in the reference's representation (lattice/src/rlwe.rs:437-487)
+        const int r = (int)ms[ph];
+        for (int q = tid; q < 2 * N; q += NT_ALL) {
+          const int k = q & (N - 1);
+          const W *y = q < N ? acc_a : acc_b;
+          const int s = k - r;
+          W rot;
+          if (s >= 0) {
+            rot = y[s];
+          } else if (s >= -N) {
+            rot = F::neg_ref(y[s + N]);
+          } else {
+            rot = y[s + 2 * N];
+          }
+          s_e[q] = F::value(F::sub(rot, y[k]));
+        }
+      } else {
+        // p = -acc.a (lattice/src/rlwe.rs:1147-1166)
+        for (int k = tid; k < N; k += NT_ALL) s_e[k] = F::value(F::neg_ref(acc_a[k]));
+      }
+      __syncthreads();
+      const uint32_t nd = ks ? nd_ks : nd_br;
+      const uint32_t bits = ks ? p.ks_bits : p.bits;
+      const uint32_t mask = (1u << bits) - 1;
+      typename F::Acc ax[V], ay[V];
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        F::acc_clear(ax[v]);
+        F::acc_clear(ay[v]);
+      }
+      for (uint32_t d = g; d < nd; d += D) {
+        const uint32_t part = ks ? 0 : d / L, j = ks ? d : d % L;
+        W x[V];
+        digits<W, V, T>(x, s_e + part * N, t, j * bits, mask);
+        NT::forward_small(x, xbuf, ping, s_tw, t, sync);
+        const W *k = ks ? p.ksk + (size_t)j * 2 * N : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          F::acc_mac(ax[v], x[v], k[v * T + t]);
+          F::acc_mac(ay[v], x[v], k[N + v * T + t]);
+        }
+      }
+      sync();  // the group's last exchange has been read: its buffers take the partial sums
+      {
+        const W off = ks ? off_ks : off_br;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          xbuf[v * T + t] = F::acc_value(ax[v], off);
+          xbuf[N + v * T + t] = F::acc_value(ay[v], off);
+        }
+      }
+      __syncthreads();
+      if (g < 2) {
+        // group 0: the a sum, group 1: the b sum over all groups' partials, then its INTT
+        W f[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          W sum = s_x[g * N + v * T + t];
+#pragma unroll 1
+          for (int h = 1; h < D; ++h) sum = F::add(sum, s_x[h * 2 * N + g * N + v * T + t]);
+          f[v] = sum;
+        }
+        // both groups have read every partial before either reuses its buffers
+        asm volatile("bar.sync 15, %0;" ::"r"(2 * T) : "memory");
+        NT::inverse(f, xbuf, ping, s_itw, t, sync);
+        if (!ks) {
+          W *y = g == 0 ? acc_a : acc_b;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const int k = NT::natural_pos(t, v);
+            y[k] = F::add(y[k], F::canon(f[v]));  // RLWE::add_assign_element_wise
+          }
+        } else {
+          // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402); b' = acc.b[0] + Q/8 + B0
+          W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const int k = NT::natural_pos(t, v);
+            const W val = F::canon(f[v]);
+            if (g == 0) {
+              if (k == 0)
+                out[0] = val;
+              else if (k >= N - (int)n + 1)
+                out[N - k] = F::neg_ref(val);
+            } else if (k == 0) {
+              const W b0 = F::canon(F::add(acc_b[0], (W)(F::P >> 3)));  // evaluate.rs:52
+              out[n] = F::canon(F::add(val, b0));
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------

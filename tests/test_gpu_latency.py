@@ -1,0 +1,63 @@
+"""Launches of at most one gate per SM take the latency form (bootstrap_dp_kernel: one gate per
+CTA, the gadget digits spread over the CTA's thread groups). Bit-exact against the oracle for every
+field and both key layouts (T = 64 and 128 threads per group), including ZAMA's 26 digits over 4
+groups and a launch of exactly one gate per SM."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(hb):
+    c = hb.Context(0)
+    yield c
+    c.close()
+
+
+def variants_for(field_id, T):
+    # a compiled gates-per-CTA variant of each (field, T) key layout
+    return {(1, 64): 4, (1, 128): 4, (0, 64): 6, (0, 128): 6, (2, 64): 6, (2, 128): 6}[(field_id, T)]
+
+
+@pytest.mark.parametrize("pid", [0, 1, 2, 3])
+@pytest.mark.parametrize("T", [64, 128])
+def test_latency_form_vs_oracle(hb, oracle, oracle_keys, ctx, pid, T):
+    from hasteboots_b200._lib import check, lib
+    params = hb.Parameters.preset(pid)
+    sk = hb.KeyGen.generate_secret_key(params, 0)
+    ev = hb.Evaluator(sk, ctx)
+    try:
+        check(lib().hb_keys_set_config(ctx.handle, ev.keys.handle, T, variants_for(params.field_id, T)),
+              "set_config", ctx.handle)
+        k = oracle_keys(pid)
+        bits = np.random.default_rng(40 + pid).integers(0, 2, (3, 5)).astype(np.uint8)
+        c = [sk.encrypt(bits[i], 900 + 10 * i) for i in range(3)]
+        for g in ("nand", "xor", "majority"):
+            if g == "majority":
+                out, ref = ev.majority(*c), oracle.gate(k, g, *c)
+            else:
+                out, ref = getattr(ev, g)(c[0], c[1]), oracle.gate(k, g, c[0], c[1])
+            assert (out == ref).all(), g
+    finally:
+        ev.keys.free()
+
+
+def test_latency_form_one_gate_per_sm(hb, oracle, oracle_keys, ctx):
+    """148 BabyBear gates: one CTA per SM, every output decrypts, sampled outputs match the oracle."""
+    sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(0), 0)
+    ev = hb.Evaluator(sk, ctx)
+    try:
+        count = 148
+        bits = np.random.default_rng(11).integers(0, 2, (2, count)).astype(np.uint8)
+        c0, c1 = sk.encrypt(bits[0], 3000), sk.encrypt(bits[1], 4000)
+        out = ev.nand(c0, c1)
+        assert (sk.decrypt(out) == 1 - (bits[0] & bits[1])).all()
+        k = oracle_keys(0)
+        pick = [0, 77, 147]
+        assert (out[pick] == oracle.gate(k, "nand", c0[pick], c1[pick])).all()
+    finally:
+        ev.keys.free()
