@@ -190,21 +190,24 @@ struct Mont32 {
   static constexpr int BITS = BB;      // bits(Q): the decomposition covers this many bits
   static constexpr int FIELD_ID = ID;
 
-  HB_HD static W canon(W x) { return x >= P ? x - P : x; }
+  // x - P when x >= P, else x, as an unsigned minimum (x - P wraps above x when x < P): one add
+  // and one min instead of a compare, a subtract and a select.
+  HB_HD static W umin(W x, W y) { return y < x ? y : x; }
+  HB_HD static W canon(W x) { return umin(x, x - P); }
   // Montgomery product a*b*2^-32 mod P for a*b < P*2^32; canonical result.
   HB_HD static W mont(W a, W b) {
     const uint64_t t = (uint64_t)a * b;
     const uint32_t m = (uint32_t)t * PINV_NEG;
     const uint64_t u = (t + (uint64_t)m * P) >> 32;
-    const uint32_t r = (uint32_t)u;
-    return r >= P ? r - P : r;
+    return canon((uint32_t)u);
   }
   HB_HD static W mul(W a, W b_mont) { return mont(a, b_mont); }
-  HB_HD static W add(W a, W b) {
-    const W s = a + b;
-    return s >= P ? s - P : s;
+  HB_HD static W add(W a, W b) { return canon(a + b); }
+  // Canonical a - b: a - b, or a - b + P when it wrapped (then a - b + P < P <= the wrapped word).
+  HB_HD static W sub(W a, W b) {
+    const W d = a - b;
+    return umin(d, d + P);
   }
-  HB_HD static W sub(W a, W b) { return a >= b ? a - b : a + P - b; }
   HB_HD static W add_c(W a, W b) { return add(a, b); }
   HB_HD static W sub_c(W a, W b) { return sub(a, b); }
   HB_HD static W neg_ref(W a) { return a == 0 ? 0 : P - a; }
