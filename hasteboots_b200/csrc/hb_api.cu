@@ -237,6 +237,18 @@ uint32_t ks_dim(const hb_params &p) {
   return m;
 }
 
+// Twiddle tables of the half-CTA groups of bootstrap_dp_kernel for keys laid out for T threads
+// (words per thread of those groups: hb::dp_wide_words).
+int dp_tables(hb_ctx *ctx, const hb_params &p, int T) {
+  if (p.ring_dim != 1024) return HB_OK;
+  const int ws = p.field_id == HB_FIELD_GOLDILOCKS ? 8 : 4;
+  const int D = ws == 8 ? 4 : 512 / T, vw = 1024 / (D / 2 * T);
+  uint32_t logv = 0;
+  while ((1 << logv) < vw) ++logv;
+  DevTables *tb;
+  return tables(ctx, p.field_id, 10, &tb, logv);
+}
+
 // Device words of the key-switching key: every n'-word chunk key polynomial spread to N words.
 size_t ksk_device_words(const hb_params &p) {
   return (size_t)(p.ring_dim / ks_dim(p)) * p.ks_len * 2 * p.ring_dim;
@@ -419,9 +431,14 @@ void boot_params(hb::BootParams<W> &prm, hb_ctx *ctx, const hb_keys *keys, const
 // Launches of at most one gate per SM (G = 1 outside the plain form) run the latency form: one gate
 // per CTA, its digits spread over the CTA's thread groups (binary LWE keys, one key-switching chunk).
 template <class F, int LOGN, int T>
-int launch_dp(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream) {
+int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t stream) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T>();
+  constexpr int LOGVW = hb::ilog2c(hb::dp_wide_words<W, N, T>());
+  // built with the keys (hb_keys_upload / hb_keys_generate / relayout), never inside a capture
+  const DevTables &tbw = ctx->tables[F::FIELD_ID][LOGN][LOGVW];
+  if (!tbw.itw) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
+  prm.itw_w = (const W *)tbw.itw;
   auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D>;
   const size_t smem = hb::dp_smem_bytes<W, N, D>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -737,6 +754,11 @@ int hb_keys_upload(hb_ctx *ctx, const hb_params *p, const void *bsk, const void 
   const std::vector<int> cand = variants(*p, k->threads_per_gate);
   if (cand.size() && std::find(cand.begin(), cand.end(), k->gates_per_cta) == cand.end())
     k->gates_per_cta = cand.back();
+  rc = dp_tables(ctx, *p, k->threads_per_gate);
+  if (rc) {
+    hb_keys_free(ctx, k);
+    return rc;
+  }
   *out = k;
   return HB_OK;
 }
@@ -1152,6 +1174,11 @@ extern "C" int hb_keys_generate(hb_ctx *ctx, const hb_params *p, uint64_t seed, 
   const std::vector<int> cand = variants(*p, k->threads_per_gate);
   if (cand.size() && std::find(cand.begin(), cand.end(), k->gates_per_cta) == cand.end())
     k->gates_per_cta = cand.back();
+  rc = dp_tables(ctx, *p, k->threads_per_gate);
+  if (rc) {
+    hb_keys_free(ctx, k);
+    return rc;
+  }
   *out = k;
   return HB_OK;
 }
@@ -1352,7 +1379,7 @@ int relayout_keys(hb_ctx *ctx, hb_keys *keys, int T) {
   keys->bsk = nbsk;
   keys->ksk = nksk;
   keys->threads_per_gate = T;
-  return HB_OK;
+  return dp_tables(ctx, keys->p, T);
 }
 
 bool compiled(const hb_params &p, int T, int G) {

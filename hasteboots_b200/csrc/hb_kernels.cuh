@@ -405,6 +405,7 @@ struct BootParams {
   const W *bsk;  // [n][pairs][2][len][2][N] slot layout, scaled (one 2N-word chunk per row)
   const W *ksk;  // [ks_chunks][ks_len][2][N] slot layout, scaled (chunk keys spread to N words)
   const W *tw, *itw;
+  const W *itw_w;  // bootstrap_dp_kernel: inverse twiddles of its half-CTA groups
   W *acc;  // unused by this kernel (accumulators live in shared memory)
   const GateJob *jobs;
   int njobs;
@@ -781,31 +782,44 @@ __host__ __device__ constexpr int dp_groups() {
   return sizeof(W) == 8 ? 4 : 512 / T;
 }
 
-// Shared memory of bootstrap_dp_kernel: twiddles (2N words), the accumulator (2N), the
-// decomposition sources E.a and E.b (2N), per group two exchange buffers (2N) that also carry the
-// group's partial sums, and the modulus-switched input.
+// Words per thread of the half-CTA groups (D/2 groups of T threads) that sum and inverse-transform
+// the a and b polynomials in bootstrap_dp_kernel.
+template <class W, int N, int T>
+__host__ __device__ constexpr int dp_wide_words() {
+  return N / (dp_groups<W, T>() / 2 * T);
+}
+
+// Shared memory of bootstrap_dp_kernel: twiddles (3N words: forward, inverse, inverse of the
+// half-CTA layout), the accumulator (2N), the decomposition sources E.a and E.b (2N), per group
+// two exchange buffers (2N) that also carry the group's partial sums, and the modulus-switched
+// input.
 template <class W, int N, int D>
 __host__ __device__ constexpr size_t dp_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(6 + 2 * D) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
+  return sizeof(W) * (size_t)(7 + 2 * D) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
 }
 
 // The same bootstrap as bootstrap_kernel (binary LWE key, one key-switching chunk) with the
 // latency of one gate cut instead of the cost of many: per blind-rotation step the 2l digit
 // polynomials of E = ACC (X^r - 1) go to D groups (digit d to group d mod D), each transforms its
 // digits and multiply-accumulates them with their key rows read straight from global memory
-// (no staging, no waits), the groups' partial sums meet in shared memory, and groups 0 and 1
-// inverse-transform the a and b sums and add them to the accumulator. The key switch spreads its
+// (no staging, no waits), the groups' partial sums meet in shared memory, and the two halves of
+// the CTA, each one group of D/2 * T threads, inverse-transform the a and b sums and add them to
+// the accumulator. The key switch spreads its
 // l_ks digits the same way. Used for launches of at most one gate per SM.
 template <class F, int LOGN, int T, int D>
 __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T>;
   constexpr int N = 1 << LOGN, V = NT::V, NT_ALL = D * T;
-  static_assert(D >= 2, "groups 0 and 1 transform the a and b sums");
+  static_assert(D >= 2 && D % 2 == 0, "two half-CTA groups transform the a and b sums");
+  constexpr int TW = D / 2 * T;  // threads of a half-CTA group
+  using NW = GroupNtt<F, LOGN, TW>;
+  constexpr int VW = NW::V;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   W *s_tw = reinterpret_cast<W *>(smem_raw);
   W *s_itw = s_tw + N;
-  W *acc_a = s_itw + N;
+  W *s_itw_w = s_itw + N;
+  W *acc_a = s_itw_w + N;
   W *acc_b = acc_a + N;
   W *s_e = acc_b + N;  // E.a then E.b (the key switch: -acc.a), natural order
   W *s_x = s_e + 2 * N;
@@ -815,11 +829,17 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
   for (int i = tid; i < N; i += NT_ALL) {
     s_tw[i] = p.tw[i];
     s_itw[i] = p.itw[i];
+    s_itw_w[i] = p.itw_w[i];
   }
   __syncthreads();
   GroupSync<T> sync{1 + g};
   W *xbuf = s_x + g * 2 * N;
   int ping = 0;
+  // half 0 (groups 0 .. D/2-1) sums and transforms the a polynomial, half 1 the b polynomial
+  const int half = g / (D / 2), tw = tid % TW;
+  GroupSync<TW> wsync{D + 1 + half};
+  W *wbuf = half == 0 ? s_e : s_x;  // free once every partial sum has been read
+  int ping_w = 0;
 
   const uint32_t n = p.n, L = p.len, two_n = 2 * N;
   // products each group accumulates per phase (digits g, g + D, ...), for the lazy offsets
@@ -929,34 +949,36 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         }
       }
       __syncthreads();
-      if (g < 2) {
-        // group 0: the a sum, group 1: the b sum over all groups' partials, then its INTT
-        W f[V];
+      {
+        // the half's sum over all groups' partials, read in its own layout: slot tw*VW + vw sits at
+        // (slot % V) * T + slot / V in a group's buffer
+        W f[VW];
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          W sum = s_x[g * N + v * T + t];
+        for (int vw = 0; vw < VW; ++vw) {
+          const int slot = tw * VW + vw;
+          const int at = half * N + (slot % V) * T + slot / V;
+          W sum = s_x[at];
 #pragma unroll 1
-          for (int h = 1; h < D; ++h) sum = F::add(sum, s_x[h * 2 * N + g * N + v * T + t]);
-          f[v] = sum;
+          for (int h = 1; h < D; ++h) sum = F::add(sum, s_x[h * 2 * N + at]);
+          f[vw] = sum;
         }
-        // both groups have read every partial before either reuses its buffers
-        asm volatile("bar.sync 15, %0;" ::"r"(2 * T) : "memory");
-        NT::inverse(f, xbuf, ping, s_itw, t, sync);
+        __syncthreads();  // every partial read: the exchange buffers are free
+        NW::inverse(f, wbuf, ping_w, s_itw_w, tw, wsync);
         if (!ks) {
-          W *y = g == 0 ? acc_a : acc_b;
+          W *y = half == 0 ? acc_a : acc_b;
 #pragma unroll
-          for (int v = 0; v < V; ++v) {
-            const int k = NT::natural_pos(t, v);
-            y[k] = F::add(y[k], F::canon(f[v]));  // RLWE::add_assign_element_wise
+          for (int vw = 0; vw < VW; ++vw) {
+            const int k = NW::natural_pos(tw, vw);
+            y[k] = F::add(y[k], F::canon(f[vw]));  // RLWE::add_assign_element_wise
           }
         } else {
           // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402); b' = acc.b[0] + Q/8 + B0
           W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
 #pragma unroll
-          for (int v = 0; v < V; ++v) {
-            const int k = NT::natural_pos(t, v);
-            const W val = F::canon(f[v]);
-            if (g == 0) {
+          for (int vw = 0; vw < VW; ++vw) {
+            const int k = NW::natural_pos(tw, vw);
+            const W val = F::canon(f[vw]);
+            if (half == 0) {
               if (k == 0)
                 out[0] = val;
               else if (k >= N - (int)n + 1)
