@@ -415,7 +415,6 @@ void boot_params(hb::BootParams<W> &prm, hb_ctx *ctx, const hb_keys *keys, const
   prm.ksk = (const W *)keys->ksk;
   prm.tw = (const W *)tb->tw;
   prm.itw = (const W *)tb->itw;
-  prm.acc = nullptr;
   prm.n = keys->p.lwe_dim;
   prm.len = keys->p.br_len;
   prm.bits = keys->p.br_bits;
@@ -429,26 +428,69 @@ void boot_params(hb::BootParams<W> &prm, hb_ctx *ctx, const hb_keys *keys, const
 }
 
 // Launches of at most one gate per SM (G = 1 outside the plain form) run the latency form: one gate
-// per CTA, its digits spread over the CTA's thread groups (binary LWE keys, one key-switching chunk).
+// per CTA, its digits spread over the CTA's thread groups (binary LWE keys, one key-switching chunk);
+// for the Goldilocks sets, whose 2l digits outnumber one CTA's groups, a cluster of kDpCluster CTAs
+// per gate while the whole launch fits the GPU's co-resident clusters.
+constexpr int kDpCluster = 4;
+
+template <class F, int LOGN, int T, int C>
+int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream, int *max_clusters) {
+  using W = typename F::W;
+  constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T>();
+  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D, C>;
+  const size_t smem = hb::dp_smem_bytes<W, N, D, C>(prm.n);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
+  if constexpr (C == 1) {
+    const unsigned grid = std::max(1u, std::min<unsigned>(prm.total_batches, (unsigned)ctx->sms));
+    kern<<<grid, D * T, smem, stream>>>(prm);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(D * T);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (max_clusters) {  // how many clusters of this shape the GPU holds at once
+      cfg.gridDim = dim3(C);
+      int m = 0;
+      e = cudaOccupancyMaxActiveClusters(&m, kern, &cfg);
+      *max_clusters = e == cudaSuccess ? m : 0;
+      return HB_OK;
+    }
+    cfg.gridDim = dim3(prm.total_batches * C);
+    e = cudaLaunchKernelEx(&cfg, kern, prm);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap cluster launch");
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
+  ctx->launches += 1;
+  return HB_OK;
+}
+
 template <class F, int LOGN, int T>
 int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t stream) {
   using W = typename F::W;
-  constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T>();
+  constexpr int N = 1 << LOGN;
   constexpr int LOGVW = hb::ilog2c(hb::dp_wide_words<W, N, T>());
   // built with the keys (hb_keys_upload / hb_keys_generate / relayout), never inside a capture
   const DevTables &tbw = ctx->tables[F::FIELD_ID][LOGN][LOGVW];
   if (!tbw.itw) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
   prm.itw_w = (const W *)tbw.itw;
-  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D>;
-  const size_t smem = hb::dp_smem_bytes<W, N, D>(prm.n);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
-  const unsigned grid = std::max(1u, std::min<unsigned>(prm.total_batches, (unsigned)ctx->sms));
-  kern<<<grid, D * T, smem, stream>>>(prm);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
-  ctx->launches += 1;
-  return HB_OK;
+  if constexpr (sizeof(W) == 8) {
+    int &m = ctx->dp_clusters[T == 128 ? 1 : 0];
+    if (m < 0) {
+      const int rc = launch_dp_c<F, LOGN, T, kDpCluster>(ctx, prm, stream, &m);
+      if (rc) return rc;
+    }
+    if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, kDpCluster>(ctx, prm, stream, nullptr);
+  }
+  return launch_dp_c<F, LOGN, T, 1>(ctx, prm, stream, nullptr);
 }
 
 template <class F, int LOGN, int T, int G, bool TERN, bool KSC>

@@ -11,7 +11,8 @@
 //                           G gates per CTA sharing every bootstrapping-key chunk, which the TMA unit
 //                           streams into a ring of shared-memory stages
 //  * bootstrap_dp_kernel    the same bootstrap for launches of at most one gate per SM: one gate
-//                           per CTA with its gadget digits spread over the CTA's thread groups
+//                           per CTA (or per cluster of CTAs) with its gadget digits spread over the
+//                           thread groups
 //  * modmul_probe_kernel    field-multiply throughput (the roofline denominator)
 #pragma once
 
@@ -406,7 +407,6 @@ struct BootParams {
   const W *ksk;  // [ks_chunks][ks_len][2][N] slot layout, scaled (chunk keys spread to N words)
   const W *tw, *itw;
   const W *itw_w;  // bootstrap_dp_kernel: inverse twiddles of its half-CTA groups
-  W *acc;  // unused by this kernel (accumulators live in shared memory)
   const GateJob *jobs;
   int njobs;
   uint32_t total_batches;
@@ -791,11 +791,28 @@ __host__ __device__ constexpr int dp_wide_words() {
 
 // Shared memory of bootstrap_dp_kernel: twiddles (3N words: forward, inverse, inverse of the
 // half-CTA layout), the accumulator (2N), the decomposition sources E.a and E.b (2N), per group
-// two exchange buffers (2N) that also carry the group's partial sums, and the modulus-switched
-// input.
-template <class W, int N, int D>
+// two exchange buffers (2N) that also carry the group's partial sums, in a cluster the CTA's
+// partial sums that the other CTAs read (2N), and the modulus-switched input.
+template <class W, int N, int D, int C>
 __host__ __device__ constexpr size_t dp_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(7 + 2 * D) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
+  return sizeof(W) * (size_t)(7 + 2 * D + (C > 1 ? 2 : 0)) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
+}
+
+// Cluster barrier halves (all threads of every CTA of the cluster, warp-uniform): arrive releases
+// this thread's shared-memory writes and reads, wait acquires every other thread's.
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// Generic address of the same shared-memory word in CTA `rank` of the cluster.
+template <class W>
+__device__ __forceinline__ const W *cluster_peer(const W *p, uint32_t rank) {
+  uint64_t in = (uint64_t)p, out;
+  asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(in), "r"(rank));
+  return reinterpret_cast<const W *>(out);
 }
 
 // The same bootstrap as bootstrap_kernel (binary LWE key, one key-switching chunk) with the
@@ -806,7 +823,13 @@ __host__ __device__ constexpr size_t dp_smem_bytes(uint32_t n) {
 // the CTA, each one group of D/2 * T threads, inverse-transform the a and b sums and add them to
 // the accumulator. The key switch spreads its
 // l_ks digits the same way. Used for launches of at most one gate per SM.
-template <class F, int LOGN, int T, int D>
+//
+// C > 1: a cluster of C CTAs (C SMs) per gate. The digits go to the C * D groups of the cluster;
+// each CTA sums its groups' partials, the CTAs read each other's sums through distributed shared
+// memory, and every CTA inverse-transforms the total itself, so every CTA keeps the same
+// accumulator without a broadcast. Two cluster barriers per phase: after the CTA sums are written,
+// and (its wait deferred to the next phase's sum) after the remote reads.
+template <class F, int LOGN, int T, int D, int C = 1>
 __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T>;
@@ -823,9 +846,13 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
   W *acc_b = acc_a + N;
   W *s_e = acc_b + N;  // E.a then E.b (the key switch: -acc.a), natural order
   W *s_x = s_e + 2 * N;
-  uint16_t *ms = reinterpret_cast<uint16_t *>(s_x + D * 2 * N);
+  W *s_cp = s_x + D * 2 * N;  // C > 1: this CTA's partial sums (a then b), read by the cluster
+  uint16_t *ms = reinterpret_cast<uint16_t *>(s_cp + (C > 1 ? 2 * N : 0));
 
   const int tid = threadIdx.x, g = tid / T, t = tid % T;
+  const uint32_t rank = C > 1 ? cluster_rank() : 0;
+  const int gg = (int)rank * D + g;  // the group's index in the cluster (digits gg, gg + C D, ...)
+  bool pending = false;              // C > 1: an arrive whose wait is still due
   for (int i = tid; i < N; i += NT_ALL) {
     s_tw[i] = p.tw[i];
     s_itw[i] = p.itw[i];
@@ -842,14 +869,14 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
   int ping_w = 0;
 
   const uint32_t n = p.n, L = p.len, two_n = 2 * N;
-  // products each group accumulates per phase (digits g, g + D, ...), for the lazy offsets
+  // products each group accumulates per phase (digits gg, gg + C D, ...), for the lazy offsets
   const uint32_t nd_br = 2 * L, nd_ks = p.ks_len;
-  const uint32_t my_br = (uint32_t)g < nd_br ? (nd_br - 1 - g) / D + 1 : 0;
-  const uint32_t my_ks = (uint32_t)g < nd_ks ? (nd_ks - 1 - g) / D + 1 : 0;
+  const uint32_t my_br = (uint32_t)gg < nd_br ? (nd_br - 1 - gg) / (C * D) + 1 : 0;
+  const uint32_t my_ks = (uint32_t)gg < nd_ks ? (nd_ks - 1 - gg) / (C * D) + 1 : 0;
   const W off_br = F::acc_offset(my_br);
   const W off_ks = F::acc_offset(my_ks);
 
-  for (uint32_t gi = blockIdx.x; gi < p.total_batches; gi += gridDim.x) {
+  for (uint32_t gi = blockIdx.x / C; gi < p.total_batches; gi += gridDim.x / C) {
     int jx = 0;
     while (jx + 1 < p.njobs && p.jobs[jx + 1].first_batch <= gi) ++jx;
     const GateJob &job = p.jobs[jx];
@@ -927,7 +954,7 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         F::acc_clear(ax[v]);
         F::acc_clear(ay[v]);
       }
-      for (uint32_t d = g; d < nd; d += D) {
+      for (uint32_t d = gg; d < nd; d += C * D) {
         const uint32_t part = ks ? 0 : d / L, j = ks ? d : d % L;
         W x[V];
         digits<W, V, T>(x, s_e + part * N, t, j * bits, mask);
@@ -953,16 +980,40 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         // the half's sum over all groups' partials, read in its own layout: slot tw*VW + vw sits at
         // (slot % V) * T + slot / V in a group's buffer
         W f[VW];
+        if constexpr (C == 1) {
 #pragma unroll
-        for (int vw = 0; vw < VW; ++vw) {
-          const int slot = tw * VW + vw;
-          const int at = half * N + (slot % V) * T + slot / V;
-          W sum = s_x[at];
+          for (int vw = 0; vw < VW; ++vw) {
+            const int slot = tw * VW + vw;
+            const int at = half * N + (slot % V) * T + slot / V;
+            W sum = s_x[at];
 #pragma unroll 1
-          for (int h = 1; h < D; ++h) sum = F::add(sum, s_x[h * 2 * N + at]);
-          f[vw] = sum;
+            for (int h = 1; h < D; ++h) sum = F::add(sum, s_x[h * 2 * N + at]);
+            f[vw] = sum;
+          }
+          __syncthreads();  // every partial read: the exchange buffers are free
+        } else {
+          if (pending) cluster_wait();  // the cluster is done reading the previous CTA sums
+          for (int q = tid; q < 2 * N; q += NT_ALL) {
+            W sum = s_x[q];
+#pragma unroll 1
+            for (int h = 1; h < D; ++h) sum = F::add(sum, s_x[h * 2 * N + q]);
+            s_cp[q] = sum;
+          }
+          cluster_arrive();
+          cluster_wait();  // every CTA's sums are written (and this CTA's buffers are read)
+#pragma unroll
+          for (int vw = 0; vw < VW; ++vw) {
+            const int slot = tw * VW + vw;
+            const int at = half * N + (slot % V) * T + slot / V;
+            // the same order of terms in every CTA, so every CTA forms the same words
+            W sum = cluster_peer(s_cp, 0)[at];
+#pragma unroll 1
+            for (uint32_t r = 1; r < (uint32_t)C; ++r) sum = F::add(sum, cluster_peer(s_cp, r)[at]);
+            f[vw] = sum;
+          }
+          cluster_arrive();  // this CTA's remote reads are done; the wait comes before the next sums
+          pending = true;
         }
-        __syncthreads();  // every partial read: the exchange buffers are free
         NW::inverse(f, wbuf, ping_w, s_itw_w, tw, wsync);
         if (!ks) {
           W *y = half == 0 ? acc_a : acc_b;
@@ -971,7 +1022,7 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
             const int k = NW::natural_pos(tw, vw);
             y[k] = F::add(y[k], F::canon(f[vw]));  // RLWE::add_assign_element_wise
           }
-        } else {
+        } else if (rank == 0) {
           // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402); b' = acc.b[0] + Q/8 + B0
           W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
 #pragma unroll
@@ -992,6 +1043,9 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
       }
       __syncthreads();
     }
+  }
+  if constexpr (C > 1) {
+    if (pending) cluster_wait();  // no CTA leaves while another may still read its shared memory
   }
 }
 

@@ -40,10 +40,11 @@ struct hb_ctx {
   std::vector<std::pair<void *, size_t>> sizes;
   std::string err;
   hbrt::DevTables tables[3][13][6];  // [field][log2 N][log2 words per thread]
-  hbrt::Scratch jobs, io, mux_tmp, acc;
+  hbrt::Scratch jobs, io, mux_tmp;
   std::atomic<unsigned long long> launches{0};  // bootstrap kernel launches issued by this context
   long long wait_limit = 0;                     // SM clock cycles per bounded wait; 0 = default
   int withhold_keys = 0;                        // test hook: bootstrap launches issue no key copies
+  int dp_clusters[2] = {-1, -1};  // co-resident latency-form clusters (Goldilocks, T = 64 / 128); -1 unknown
 };
 
 struct hb_keys {

@@ -61,3 +61,21 @@ def test_latency_form_one_gate_per_sm(hb, oracle, oracle_keys, ctx):
         assert (out[pick] == oracle.gate(k, "nand", c0[pick], c1[pick])).all()
     finally:
         ev.keys.free()
+
+
+@pytest.mark.parametrize("count", [3, 100])
+def test_latency_form_goldilocks_cluster_and_single_sm(hb, oracle, oracle_keys, ctx, count):
+    """Goldilocks launches small enough for a cluster of CTAs per gate (3 gates) and beyond the
+    GPU's co-resident clusters (100 gates: one SM per gate) against the oracle."""
+    sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(1), 0)
+    ev = hb.Evaluator(sk, ctx)
+    try:
+        bits = np.random.default_rng(70 + count).integers(0, 2, (2, count)).astype(np.uint8)
+        c0, c1 = sk.encrypt(bits[0], 7000), sk.encrypt(bits[1], 8000)
+        out = ev.nand(c0, c1)
+        assert (sk.decrypt(out) == 1 - (bits[0] & bits[1])).all()
+        k = oracle_keys(1)
+        pick = sorted({0, count // 2, count - 1})
+        assert (out[pick] == oracle.gate(k, "nand", c0[pick], c1[pick])).all()
+    finally:
+        ev.keys.free()
