@@ -791,11 +791,11 @@ __host__ __device__ constexpr int dp_wide_words() {
 
 // Shared memory of bootstrap_dp_kernel: twiddles (3N words: forward, inverse, inverse of the
 // half-CTA layout), the accumulator (2N), the decomposition sources E.a and E.b (2N), per group
-// two exchange buffers (2N) that also carry the group's partial sums, in a cluster the CTA's
-// partial sums that the other CTAs read (2N), and the modulus-switched input.
+// two exchange buffers (2N) that also carry the group's partial sums, in a cluster two buffers of
+// the CTA's partial sums that the other CTAs read (2 x 2N), and the modulus-switched input.
 template <class W, int N, int D, int C>
 __host__ __device__ constexpr size_t dp_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(7 + 2 * D + (C > 1 ? 2 : 0)) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
+  return sizeof(W) * (size_t)(7 + 2 * D + (C > 1 ? 4 : 0)) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
 }
 
 // Cluster barrier halves (all threads of every CTA of the cluster, warp-uniform): arrive releases
@@ -827,8 +827,10 @@ __device__ __forceinline__ const W *cluster_peer(const W *p, uint32_t rank) {
 // C > 1: a cluster of C CTAs (C SMs) per gate. The digits go to the C * D groups of the cluster;
 // each CTA sums its groups' partials, the CTAs read each other's sums through distributed shared
 // memory, and every CTA inverse-transforms the total itself, so every CTA keeps the same
-// accumulator without a broadcast. Two cluster barriers per phase: after the CTA sums are written,
-// and (its wait deferred to the next phase's sum) after the remote reads.
+// accumulator without a broadcast. One cluster barrier per phase, after the CTA sums are written:
+// the sums alternate between two buffers, and a CTA passes phase k's barrier only after every CTA
+// arrived there, that is after every CTA finished reading phase k-1's sums, so the buffer written
+// in phase k+1 is free. A last barrier keeps every CTA until the others have read its sums.
 template <class F, int LOGN, int T, int D, int C = 1>
 __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
@@ -846,13 +848,13 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
   W *acc_b = acc_a + N;
   W *s_e = acc_b + N;  // E.a then E.b (the key switch: -acc.a), natural order
   W *s_x = s_e + 2 * N;
-  W *s_cp = s_x + D * 2 * N;  // C > 1: this CTA's partial sums (a then b), read by the cluster
-  uint16_t *ms = reinterpret_cast<uint16_t *>(s_cp + (C > 1 ? 2 * N : 0));
+  W *s_cp = s_x + D * 2 * N;  // C > 1: this CTA's partial sums (a then b) x 2, read by the cluster
+  uint16_t *ms = reinterpret_cast<uint16_t *>(s_cp + (C > 1 ? 4 * N : 0));
 
   const int tid = threadIdx.x, g = tid / T, t = tid % T;
   const uint32_t rank = C > 1 ? cluster_rank() : 0;
   const int gg = (int)rank * D + g;  // the group's index in the cluster (digits gg, gg + C D, ...)
-  bool pending = false;              // C > 1: an arrive whose wait is still due
+  uint32_t cp_turn = 0;              // C > 1: which sum buffer this phase writes
   for (int i = tid; i < N; i += NT_ALL) {
     s_tw[i] = p.tw[i];
     s_itw[i] = p.itw[i];
@@ -992,27 +994,26 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
           }
           __syncthreads();  // every partial read: the exchange buffers are free
         } else {
-          if (pending) cluster_wait();  // the cluster is done reading the previous CTA sums
+          W *cp = s_cp + (cp_turn & 1) * 2 * N;
+          ++cp_turn;
           for (int q = tid; q < 2 * N; q += NT_ALL) {
             W sum = s_x[q];
 #pragma unroll 1
             for (int h = 1; h < D; ++h) sum = F::add(sum, s_x[h * 2 * N + q]);
-            s_cp[q] = sum;
+            cp[q] = sum;
           }
           cluster_arrive();
-          cluster_wait();  // every CTA's sums are written (and this CTA's buffers are read)
+          cluster_wait();  // every CTA's sums are written (and this CTA's group buffers are read)
 #pragma unroll
           for (int vw = 0; vw < VW; ++vw) {
             const int slot = tw * VW + vw;
             const int at = half * N + (slot % V) * T + slot / V;
             // the same order of terms in every CTA, so every CTA forms the same words
-            W sum = cluster_peer(s_cp, 0)[at];
+            W sum = cluster_peer(cp, 0)[at];
 #pragma unroll 1
-            for (uint32_t r = 1; r < (uint32_t)C; ++r) sum = F::add(sum, cluster_peer(s_cp, r)[at]);
+            for (uint32_t r = 1; r < (uint32_t)C; ++r) sum = F::add(sum, cluster_peer(cp, r)[at]);
             f[vw] = sum;
           }
-          cluster_arrive();  // this CTA's remote reads are done; the wait comes before the next sums
-          pending = true;
         }
         NW::inverse(f, wbuf, ping_w, s_itw_w, tw, wsync);
         if (!ks) {
@@ -1044,8 +1045,9 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
       __syncthreads();
     }
   }
-  if constexpr (C > 1) {
-    if (pending) cluster_wait();  // no CTA leaves while another may still read its shared memory
+  if constexpr (C > 1) {  // no CTA leaves while another may still read its shared memory
+    cluster_arrive();
+    cluster_wait();
   }
 }
 
