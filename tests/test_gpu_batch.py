@@ -3,7 +3,10 @@
 import numpy as np
 import pytest
 
+from conftest import hb_params_of
 from gpu_util import empty_dev, from_dev, to_dev
+
+SETS = [0, 1, 2, 3, 4, 100]  # the five presets and the ternary-LWE-key set
 
 pytestmark = pytest.mark.gpu
 
@@ -18,8 +21,8 @@ def ctx(hb):
 @pytest.fixture(scope="module")
 def evaluators(hb, ctx):
     evs = {}
-    for pid in (0, 1, 2):
-        sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(pid), 0)
+    for pid in SETS:
+        sk = hb.KeyGen.generate_secret_key(hb_params_of(hb, pid), 0)
         evs[pid] = (sk, hb.Evaluator(sk, ctx))
     yield evs
     for sk, ev in evs.values():
@@ -58,8 +61,8 @@ def test_mixed_batch_equals_alone(hb, evaluators, ctx):
     rng = np.random.default_rng(4)
     gates = ["nand", "and", "or", "xor", "xnor", "nor", "majority"]
     plan = []
-    for i in range(9):
-        pid = int(rng.integers(0, 3))
+    for i in range(12):
+        pid = SETS[int(rng.integers(0, len(SETS)))]
         count = int(np.exp(rng.uniform(0, np.log(300))))
         gate = gates[i % len(gates)]
         plan.append((pid, gate, max(1, count)))

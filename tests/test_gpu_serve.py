@@ -4,15 +4,19 @@ across parameter sets, with admission against an HBM budget."""
 import numpy as np
 import pytest
 
+from conftest import hb_params_of
+
 pytestmark = pytest.mark.gpu
+
+SETS = [0, 1, 2, 3, 4, 100]  # the five presets and the ternary-LWE-key set
 
 
 @pytest.fixture(scope="module")
 def setup(hb):
     ctx = hb.Context(0)
     evs = {}
-    for pid in (0, 1, 2):
-        sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(pid), 0)
+    for pid in SETS:
+        sk = hb.KeyGen.generate_secret_key(hb_params_of(hb, pid), 0)
         evs[pid] = (sk, hb.Evaluator(sk, ctx))
     yield ctx, evs
     for sk, ev in evs.values():
@@ -24,7 +28,7 @@ def _plan(evs, n, seed):
     rng = np.random.default_rng(seed)
     reqs = []
     for i in range(n):
-        pid = int(rng.integers(0, 3))
+        pid = SETS[int(rng.integers(0, len(SETS)))]
         count = int(np.exp(rng.uniform(0, np.log(200))))
         gate = ["nand", "and", "xor", "majority"][i % 4]
         sk, ev = evs[pid]
