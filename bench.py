@@ -431,18 +431,21 @@ def workload_serve(args):
 
 
 def workload_single(args):
-    """One BabyBear NAND gate (config 1): latency of one hb_gate_device call (the latency form: one
-    CTA whose thread groups share the gate's digits), with the plain form (one kernel launch of a
-    single 64-thread group) beside it."""
+    """One NAND gate (config 1: BABYBEAR_BINARY_128_BITS; --single-preset picks another set):
+    latency of one hb_gate_device call (the latency form: one CTA -- for the Goldilocks sets a
+    cluster of CTAs -- whose thread groups share the gate's digits), with the plain form (one kernel
+    launch of a single thread group) beside it."""
     import torch
     from hasteboots_b200 import tfhe
     from hasteboots_b200._lib import check, lib
-    sk = tfhe.KeyGen.generate_secret_key(tfhe.Parameters.preset(0), 0)
+    params = tfhe.Parameters.preset(args.single_preset)
+    sk = tfhe.KeyGen.generate_secret_key(params, 0)
     ctx = tfhe.Context(0)
     ev = tfhe.Evaluator(sk, ctx)
     c0, c1 = sk.encrypt([1], 0), sk.encrypt([1], 1)
-    d0 = torch.from_numpy(c0.view(np.int32).copy()).cuda()
-    d1 = torch.from_numpy(c1.view(np.int32).copy()).cuda()
+    ivt = np.int64 if params.dtype == np.uint64 else np.int32
+    d0 = torch.from_numpy(c0.view(ivt).copy()).cuda()
+    d1 = torch.from_numpy(c1.view(ivt).copy()).cuda()
     do = torch.zeros_like(d0)
     dp = torch.zeros_like(d0)
     torch.cuda.synchronize()
@@ -456,16 +459,19 @@ def workload_single(args):
         plain()
     times = [_timed(stream, gate, 1) for _ in range(args.steps)]
     ptimes = [_timed(stream, plain, 1) for _ in range(args.steps)]
-    out = do.cpu().numpy().view(np.uint32)
+    out = do.cpu().numpy().view(params.dtype)
     bit = sk.decrypt(out)[0]
-    same = bool((out == dp.cpu().numpy().view(np.uint32)).all())
-    line = {"metric": "single NAND bootstrap latency, BABYBEAR_BINARY_128_BITS", "value": float(np.median(times)),
+    same = bool((out == dp.cpu().numpy().view(params.dtype)).all())
+    line = {"metric": "single NAND bootstrap latency, " + params.name.replace("_PARAMETERS", ""),
+            "value": float(np.median(times)),
             "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "dtype": "u32", "data": "synthetic (seed-0 keys)",
+            "warmup": args.warmup, "dtype": "u64" if params.dtype == np.uint64 else "u32",
+            "data": "synthetic (seed-0 keys)",
             "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
             "plain_form_ms": {"p50": float(np.percentile(ptimes, 50)), "p99": float(np.percentile(ptimes, 99))},
-            "config": {"workload": "1 NAND gate through hb_gate_device: one CTA of 8 thread groups sharing the "
-                                   "gate's digits; plain form: one launch of one 64-thread group"},
+            "config": {"workload": "1 NAND gate through hb_gate_device (the latency form: the gate's digits "
+                                   "over the thread groups of one CTA, or of a 4-CTA cluster for the "
+                                   "Goldilocks sets); plain form: one launch of one thread group"},
             "checks": {"nand(1,1)=0": bool(bit == 0), "equals_plain_form": same}}
     print(json.dumps(line), flush=True)
     ev.keys.free()
@@ -486,6 +492,8 @@ def main():
     ap.add_argument("--preset", type=int, default=PRESET,
                     help="0 BABYBEAR, 1 GOLDILOCKS (default, the headline workload), 2 ZAMA, "
                          "3 DEFAULT_TERNARY, 4 CUSTOM_TERNARY")
+    ap.add_argument("--single-preset", type=int, default=0,
+                    help="single: the parameter set of the one gate (default 0, BABYBEAR)")
     ap.add_argument("--workload", default="gates", choices=["gates", "mixed", "ntt", "single", "serve"],
                     help="gates: 16384 NAND gates (default, the contract line); mixed: 64 jobs across "
                          "the three sets in one graph; ntt: NTT/external-product microbench; single: "
