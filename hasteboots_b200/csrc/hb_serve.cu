@@ -64,6 +64,8 @@ struct Wave {
   bool failed = false;  // a launch of this wave failed: its requests complete as failed
 };
 
+// Key sets per wave (one persistent launch, on its own stream, per key set): wave selection leaves
+// the requests of a further set for the next wave.
 constexpr int kMaxSets = 4;
 
 }  // namespace
@@ -161,7 +163,12 @@ int launch_wave(hb_server *s, std::vector<Request *> reqs, int slot) {
                    r->nin > 2 ? b + 2 * r->lwe_bytes : nullptr, b + r->nin * r->lwe_bytes, r->count, &j);
     tabs[k].push_back(j);
   }
-  if ((int)sets.size() > kMaxSets) return HB_ERR_UNSUPPORTED;
+  if ((int)sets.size() > kMaxSets) {  // wave selection never takes more sets; fail rather than strand
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (Request *r : reqs) fail_request(s, r);
+    s->cv_done.notify_all();
+    return HB_ERR_UNSUPPORTED;
+  }
   cudaEvent_t fork;
   cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
   cudaEventRecord(fork, ws);
@@ -270,12 +277,18 @@ void worker_main(hb_server *s) {
         if (!used) break;
       }
       std::vector<Request *> take;
+      std::vector<hb_keys *> keysets;
       uint64_t gates = 0;
       size_t i = 0;
       for (; i < s->ready.size(); ++i) {
-        if (!take.empty() && s->cfg.max_wave_gates && gates + s->ready[i]->count > s->cfg.max_wave_gates) break;
-        take.push_back(s->ready[i]);
-        gates += s->ready[i]->count;
+        Request *r = s->ready[i];
+        if (!take.empty() && s->cfg.max_wave_gates && gates + r->count > s->cfg.max_wave_gates) break;
+        if (std::find(keysets.begin(), keysets.end(), r->keys) == keysets.end()) {
+          if ((int)keysets.size() == kMaxSets) break;  // the next set starts the next wave
+          keysets.push_back(r->keys);
+        }
+        take.push_back(r);
+        gates += r->count;
       }
       s->ready.erase(s->ready.begin(), s->ready.begin() + i);
       int rc = launch_wave(s, take, slot);
