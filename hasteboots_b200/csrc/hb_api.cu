@@ -428,16 +428,16 @@ void boot_params(hb::BootParams<W> &prm, hb_ctx *ctx, const hb_keys *keys, const
 }
 
 // Launches of at most one gate per SM (G = 1 outside the plain form) run the latency form: one gate
-// per CTA, its digits spread over the CTA's thread groups (binary LWE keys, one key-switching chunk);
+// per CTA, its digits spread over the CTA's thread groups (binary LWE keys);
 // for the Goldilocks sets, whose 2l digits outnumber one CTA's groups, a cluster of kDpCluster CTAs
 // per gate while the whole launch fits the GPU's co-resident clusters.
 constexpr int kDpCluster = 4;
 
-template <class F, int LOGN, int T, int C>
+template <class F, int LOGN, int T, int C, bool KSC>
 int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream, int *max_clusters) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T>();
-  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D, C>;
+  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D, C, KSC>;
   const size_t smem = hb::dp_smem_bytes<W, N, D, C>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
@@ -473,7 +473,7 @@ int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStrea
   return HB_OK;
 }
 
-template <class F, int LOGN, int T>
+template <class F, int LOGN, int T, bool KSC>
 int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t stream) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
@@ -484,13 +484,13 @@ int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t strea
   prm.itw_w = (const W *)tbw.itw;
   if constexpr (sizeof(W) == 8) {
     int &m = ctx->dp_clusters[T == 128 ? 1 : 0];
-    if (m < 0) {
-      const int rc = launch_dp_c<F, LOGN, T, kDpCluster>(ctx, prm, stream, &m);
+    if (m < 0) {  // the same shared memory and threads with or without KSC
+      const int rc = launch_dp_c<F, LOGN, T, kDpCluster, KSC>(ctx, prm, stream, &m);
       if (rc) return rc;
     }
-    if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, kDpCluster>(ctx, prm, stream, nullptr);
+    if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, kDpCluster, KSC>(ctx, prm, stream, nullptr);
   }
-  return launch_dp_c<F, LOGN, T, 1>(ctx, prm, stream, nullptr);
+  return launch_dp_c<F, LOGN, T, 1, KSC>(ctx, prm, stream, nullptr);
 }
 
 template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
@@ -527,7 +527,7 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
     prm.jobs = djobs;
     prm.njobs = (int)jobs.size();
     prm.total_batches = batches;
-    if constexpr (G == 1 && !TERN && !KSC) return launch_dp<F, LOGN, T>(ctx, prm, ctx->stream);
+    if constexpr (G == 1 && !TERN) return launch_dp<F, LOGN, T, KSC>(ctx, prm, ctx->stream);
     kern<<<grid, block, smem, ctx->stream>>>(prm);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
@@ -621,7 +621,7 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
   prm.jobs = djobs;
   prm.njobs = njobs;
   prm.total_batches = batches;
-  if constexpr (G == 1 && !TERN && !KSC) return launch_dp<F, LOGN, T>(ctx, prm, stream);
+  if constexpr (G == 1 && !TERN) return launch_dp<F, LOGN, T, KSC>(ctx, prm, stream);
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);

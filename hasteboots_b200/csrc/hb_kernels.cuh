@@ -831,7 +831,11 @@ __device__ __forceinline__ const W *cluster_peer(const W *p, uint32_t rank) {
 // the sums alternate between two buffers, and a CTA passes phase k's barrier only after every CTA
 // arrived there, that is after every CTA finished reading phase k-1's sums, so the buffer written
 // in phase k+1 is free. A last barrier keeps every CTA until the others have read its sums.
-template <class F, int LOGN, int T, int D, int C = 1>
+//
+// KSC: the key switch in ks_chunks chunks of n' < N words (as bootstrap_kernel's KSC): digit d of
+// the key-switch phase is digit d mod l_ks of chunk d / l_ks, whose source words are formed from
+// the accumulator where the digit is taken, and the extraction reads every (N/n')-th coefficient.
+template <class F, int LOGN, int T, int D, int C = 1, bool KSC = false>
 __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T>;
@@ -872,7 +876,7 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
 
   const uint32_t n = p.n, L = p.len, two_n = 2 * N;
   // products each group accumulates per phase (digits gg, gg + C D, ...), for the lazy offsets
-  const uint32_t nd_br = 2 * L, nd_ks = p.ks_len;
+  const uint32_t nd_br = 2 * L, nd_ks = (KSC ? p.ks_chunks : 1) * p.ks_len;
   const uint32_t my_br = (uint32_t)gg < nd_br ? (nd_br - 1 - gg) / (C * D) + 1 : 0;
   const uint32_t my_ks = (uint32_t)gg < nd_ks ? (nd_ks - 1 - gg) / (C * D) + 1 : 0;
   const W off_br = F::acc_offset(my_br);
@@ -942,7 +946,7 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
           }
           s_e[q] = F::value(F::sub(rot, y[k]));
         }
-      } else {
+      } else if (!KSC) {
         // p = -acc.a (lattice/src/rlwe.rs:1147-1166)
         for (int k = tid; k < N; k += NT_ALL) s_e[k] = F::value(F::neg_ref(acc_a[k]));
       }
@@ -957,11 +961,32 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         F::acc_clear(ay[v]);
       }
       for (uint32_t d = gg; d < nd; d += C * D) {
-        const uint32_t part = ks ? 0 : d / L, j = ks ? d : d % L;
+        const uint32_t part = ks ? 0 : d / L, j = ks ? d % p.ks_len : d % L;
         W x[V];
-        digits<W, V, T>(x, s_e + part * N, t, j * bits, mask);
+        if (KSC && ks) {
+          // chunk c of the permuted -acc.a (fhe_core/src/key_switch/rlwe.rs:123-131), word u at
+          // slot u * stride: -a[N - c n'] for u = 0 (a[0] negated twice for c = 0), else
+          // a[N - (c + 1) n' + u], then negated
+          const uint32_t c = d / p.ks_len, kn = p.ks_n, stride = N / kn;
+          W e[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const uint32_t k = (uint32_t)NT::natural_pos(t, v);
+            W w = 0;
+            if (k % stride == 0) {
+              const uint32_t u = k / stride;
+              const W a = u != 0 ? acc_a[N - (c + 1) * kn + u]
+                                 : (c == 0 ? F::neg_ref(F::neg_ref(acc_a[0])) : F::neg_ref(acc_a[N - c * kn]));
+              w = F::value(F::neg_ref(a));
+            }
+            e[v] = w;
+          }
+          digits_reg<W, V>(x, e, j * bits, mask);
+        } else {
+          digits<W, V, T>(x, s_e + part * N, t, j * bits, mask);
+        }
         NT::forward_small(x, xbuf, ping, s_tw, t, sync);
-        const W *k = ks ? p.ksk + (size_t)j * 2 * N : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
+        const W *k = ks ? p.ksk + (size_t)d * 2 * N : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
 #pragma unroll
         for (int v = 0; v < V; ++v) {
           F::acc_mac(ax[v], x[v], k[v * T + t]);
@@ -1024,17 +1049,22 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
             y[k] = F::add(y[k], F::canon(f[vw]));  // RLWE::add_assign_element_wise
           }
         } else if (rank == 0) {
-          // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402); b' = acc.b[0] + Q/8 + B0
+          // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402); b' = acc.b[0] + Q/8 + B0; with
+          // KSC the n'-word result sits at every (N/n')-th slot
           W *out = reinterpret_cast<W *>(job.out) + gate * lwe_words;
+          const int kn = KSC ? (int)p.ks_n : N, ks_stride = N / kn;
 #pragma unroll
           for (int vw = 0; vw < VW; ++vw) {
             const int k = NW::natural_pos(tw, vw);
             const W val = F::canon(f[vw]);
             if (half == 0) {
-              if (k == 0)
-                out[0] = val;
-              else if (k >= N - (int)n + 1)
-                out[N - k] = F::neg_ref(val);
+              if (!KSC || k % ks_stride == 0) {
+                const int u = KSC ? k / ks_stride : k;
+                if (u == 0)
+                  out[0] = val;
+                else if (u >= kn - (int)n + 1)
+                  out[kn - u] = F::neg_ref(val);
+              }
             } else if (k == 0) {
               const W b0 = F::canon(F::add(acc_b[0], (W)(F::P >> 3)));  // evaluate.rs:52
               out[n] = F::canon(F::add(val, b0));
