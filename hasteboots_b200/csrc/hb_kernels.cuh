@@ -986,12 +986,15 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
           digits<W, V, T>(x, s_e + part * N, t, j * bits, mask);
         }
         const W *k = ks ? p.ksk + (size_t)d * 2 * N : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
-        // start the key row's way from HBM into L2 while the digit transform runs (the loads below
-        // come after the transform's barriers, so they cannot be issued earlier)
+        // Goldilocks keys (191-310 MB) exceed L2: start the key row's way from HBM into L2 while the
+        // digit transform runs (the loads below come after the transform's barriers, so they cannot
+        // be issued earlier). The 32-bit sets' keys stay in L2, where this only costs instructions.
+        if constexpr (sizeof(W) == 8) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(k + v * T + t));
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(k + N + v * T + t));
+          for (int v = 0; v < V; ++v) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(k + v * T + t));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(k + N + v * T + t));
+          }
         }
         NT::forward_small(x, xbuf, ping, s_tw, t, sync);
 #pragma unroll
