@@ -988,7 +988,8 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         const W *k = ks ? p.ksk + (size_t)d * 2 * N : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
         // Goldilocks keys (191-310 MB) exceed L2: start the key row's way from HBM into L2 while the
         // digit transform runs (the loads below come after the transform's barriers, so they cannot
-        // be issued earlier). The 32-bit sets' keys stay in L2, where this only costs instructions.
+        // be issued earlier). Measured for the Goldilocks sets; BabyBear's 48 MB key stays in L2,
+        // where it only cost instructions, so the 32-bit sets go without it.
         if constexpr (sizeof(W) == 8) {
 #pragma unroll
           for (int v = 0; v < V; ++v) {
