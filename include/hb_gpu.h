@@ -158,8 +158,9 @@ int hb_keys_download(hb_ctx *ctx, const hb_keys *keys, void *bsk, size_t bsk_wor
  * (tfhe/src/bfhe/evaluate.rs:98-262). c2 is read by MAJORITY and MUX only. Host buffers. */
 int hb_gate(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1, const void *c2,
             void *out, size_t count);
-/* Same on device buffers, enqueued on the context stream (one persistent launch per bootstrap
- * layer: MUX takes two). */
+/* Same on device buffers, enqueued on the context stream (one launch per bootstrap layer: MUX takes
+ * two). A layer of at most one gate per SM runs the latency form -- one CTA per gate, or for the
+ * Goldilocks sets a cluster of 4 CTAs per gate -- and larger layers the persistent batched kernel. */
 int hb_gate_device(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1,
                    const void *c2, void *out, size_t count);
 /* The plain form: one kernel launch per gate. */
@@ -219,13 +220,14 @@ typedef struct hb_job {
 } hb_job;
 typedef struct hb_batch hb_batch;
 
-/* Plans a batch of jobs that may mix parameter sets and gate kinds: one persistent launch per key
- * set, SMs split across sets by estimated work, all captured into one CUDA graph. */
+/* Plans a batch of jobs that may mix parameter sets and gate kinds: one launch per key set on its own
+ * stream, each with a full grid (the block scheduler hands SMs to the next set's CTAs as the previous
+ * set's retire), all captured into one CUDA graph. */
 int hb_batch_create(hb_ctx *ctx, const hb_job *jobs, size_t njobs, hb_batch **out);
 /* Enqueues the whole batch as one graph launch on the context stream. */
 int hb_batch_launch(hb_ctx *ctx, hb_batch *batch);
 void hb_batch_free(hb_ctx *ctx, hb_batch *batch);
-/* Gates in the batch, kernels per launch, and the SM share of each (up to grid_cap entries). */
+/* Gates in the batch, kernels per launch, and the grid of each (up to grid_cap entries). */
 int hb_batch_info(const hb_batch *batch, uint64_t *gates, int *launches, int *grid, int grid_cap);
 
 /* ---- serving: request loop with continuous batching ----------------------------------------
@@ -271,12 +273,13 @@ int hb_serve_stop(hb_server *s);
  * device memory from its own pool. No counterpart in the reference.
  * The intermediate ciphertexts, job table and status word live in a 16 MiB array compiled into the
  * library, which every GPU that loads the library holds until the process exits. count is at most
- * (16 MiB - 1 KiB) / (2 (n + 1) word bytes): 1438 gates for the Goldilocks sets, 2876 for BabyBear;
- * larger counts return HB_ERR_INVALID. The first call on a device looks up the array's device
- * address, so make that call before any stream capture. Every call uses the same array: calls whose
- * work overlaps on the GPU (other streams, contexts or host threads) race and must be serialised.
- * Device pointers in; returns when `out` holds the result (synchronises the context stream).
- * The keys must have been uploaded on this context. */
+ * (16 MiB - 1 KiB) / (2 (n + 1) word bytes): 1438 gates for the Goldilocks sets, 2876 for BabyBear,
+ * 2045 for DEFAULT_TERNARY, 4087 for CUSTOM_TERNARY; larger counts return HB_ERR_INVALID. The
+ * first call on a device looks up the array's device address, so make that call before any stream
+ * capture. Every call uses the same array: calls whose work overlaps on the GPU (other streams,
+ * contexts or host threads) race and must be serialised. Device pointers in; returns when `out`
+ * holds the result (synchronises the context stream). The keys must have been created (uploaded or
+ * generated) on this context. */
 int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void *c0, const void *c1,
                                const void *c2, void *out, size_t count);
 
@@ -286,7 +289,7 @@ int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void *c0, const
  * integer-pipe ceiling against which bootstrapping's modular multiplies are measured. No
  * counterpart in the reference, which publishes CPU timings only. */
 int hb_probe_modmul(hb_ctx *ctx, int field_id, double *modmul_per_s);
-/* Kernel launches the context has issued for bootstrapping (batched and plain forms). */
+/* Kernel launches the context has issued for bootstrapping (batched, latency and plain forms). */
 uint64_t hb_ctx_launches(const hb_ctx *ctx);
 /* Limit, in SM clock cycles, of every bounded wait inside this context's kernels (waits for key
  * chunks in flight); 0 restores the default (about 2 s). A wait that runs out makes the call return
