@@ -483,10 +483,12 @@ int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t strea
   if (!tbw.itw) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
   prm.itw_w = (const W *)tbw.itw;
   if constexpr (sizeof(W) == 8) {
-    int &m = ctx->dp_clusters[T == 128 ? 1 : 0];
+    std::atomic<int> &cached = ctx->dp_clusters[T == 128 ? 1 : 0];
+    int m = cached.load();
     if (m < 0) {  // the same shared memory and threads with or without KSC
       const int rc = launch_dp_c<F, LOGN, T, kDpCluster, KSC>(ctx, prm, stream, &m);
       if (rc) return rc;
+      cached.store(m);
     }
     if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, kDpCluster, KSC>(ctx, prm, stream, nullptr);
   }

@@ -44,7 +44,9 @@ struct hb_ctx {
   std::atomic<unsigned long long> launches{0};  // bootstrap kernel launches issued by this context
   long long wait_limit = 0;                     // SM clock cycles per bounded wait; 0 = default
   int withhold_keys = 0;                        // test hook: bootstrap launches issue no key copies
-  int dp_clusters[2] = {-1, -1};  // co-resident latency-form clusters (Goldilocks, T = 64 / 128); -1 unknown
+  // co-resident latency-form clusters (Goldilocks, T = 64 / 128); -1 unknown. Atomic: the serving
+  // loop's worker thread launches on the context too.
+  std::atomic<int> dp_clusters[2] = {-1, -1};
 };
 
 struct hb_keys {
