@@ -37,24 +37,36 @@ def _run(cmd):
     subprocess.run(cmd, check=True)
 
 
+def _run_all(cmds):
+    """Runs the compile commands concurrently; raises if any fails."""
+    procs = []
+    for cmd in cmds:
+        print(" ".join(cmd), flush=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+
+
 def build(force=False, verbose_ptxas=False):
     if not force and up_to_date():
         return OUT
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in CU_SOURCES:
         obj = os.path.join(BUILD, src + ".o")
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
                "-Xcompiler", "-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = os.path.join(BUILD, src + ".o")
-        _run([CXX, "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-fno-fast-math",
-              "-I", "/usr/local/cuda/include", "-c", os.path.join(CSRC, src), "-o", obj])
+        cmds.append([CXX, "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-fno-fast-math",
+                     "-I", "/usr/local/cuda/include", "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    _run_all(cmds)
     tmp = OUT + ".tmp"
     _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-lpthread"])
     os.replace(tmp, OUT)
