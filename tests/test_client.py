@@ -34,6 +34,25 @@ def test_chunked_key_switching_key_matches_oracle(hb, oracle_keys, pid):
     assert (bsk == k.bsk).all() and (ksk == k.ksk).all()
 
 
+@pytest.mark.parametrize("pid", [0, 1, 4])
+def test_cbd_keygen_matches_oracle(hb, oracle, pid):
+    """sigma exactly 3.2 selects the centered binomial sampler for the RGSW and key-switching error
+    polynomials (algebra/src/random.rs:91-92); the product's generator and the oracle's agree on
+    every field, including the release-build wrap of its a < b branch."""
+    from hasteboots_b200._lib import HbParams
+    base = hb.Parameters.preset(pid)
+    raw = HbParams.from_buffer_copy(base.raw)
+    raw.ring_noise_std = 3.2
+    raw.ks_noise_std = 3.2
+    p = hb.Parameters(raw, base.name + "+cbd")
+    bsk, ksk = hb.KeyGen.generate_secret_key(p, 3).evaluation_key_material()
+    op = oracle.preset(pid)
+    op.ring_noise_std = 3.2
+    op.ks_noise_std = 3.2
+    k = oracle.keygen(op, 3)
+    assert (bsk == k.bsk).all() and (ksk == k.ksk).all()
+
+
 @pytest.mark.parametrize("pid", ALL_SETS)
 def test_encrypt_decrypt_matches_oracle(hb, oracle, oracle_keys, pid):
     p = hb_params_of(hb, pid)

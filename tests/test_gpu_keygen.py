@@ -37,6 +37,28 @@ def test_device_keygen_equals_host_keygen_and_upload(hb, ctx, pid):
         gen.free()
 
 
+@pytest.mark.parametrize("pid", [0, 1, 4])
+def test_device_keygen_cbd_noise_equals_host(hb, ctx, pid):
+    """sigma exactly 3.2: the device generator's centered binomial noise equals the host's."""
+    from hasteboots_b200._lib import HbParams
+    base = hb.Parameters.preset(pid)
+    raw = HbParams.from_buffer_copy(base.raw)
+    raw.ring_noise_std = 3.2
+    raw.ks_noise_std = 3.2
+    params = hb.Parameters(raw, base.name + "+cbd")
+    sk = hb.KeyGen.generate_secret_key(params, 3)
+    bsk, ksk = sk.evaluation_key_material()
+    up = hb.DeviceKeys(ctx, params, bsk, ksk)
+    gen, _, _ = hb.DeviceKeys.generate(ctx, params, 3)
+    try:
+        b_up, k_up = up.download()
+        b_gen, k_gen = gen.download()
+        assert (b_gen == b_up).all() and (k_gen == k_up).all()
+    finally:
+        up.free()
+        gen.free()
+
+
 @pytest.mark.parametrize("pid", [0, 1, 3, 100])
 def test_device_encrypt_equals_host(hb, ctx, pid):
     from hasteboots_b200._lib import check, lib
