@@ -443,7 +443,9 @@ __host__ __device__ constexpr int boot_stages() {
 }
 
 // TERN: ternary LWE key (TernaryBlindRotationKey, fhe_core/src/blind_rotation/rlwe/ternary.rs:26-119)
-// with two RGSWs per key coefficient, for fields whose words stay canonical.
+// with two RGSWs per key coefficient, for fields whose words stay canonical. E = (X^a_i - 1) ACC is
+// the product the reference's comment names (ternary.rs:91); its code forms it from an
+// untransformed NTT-domain monomial (:93-100), which this kernel does not reproduce.
 // KSC: key switch in ks_chunks chunks of n' = next_pow2(n) < N words; without it the key switch is
 // the single chunk n' = N of the reference presets, with no chunk bookkeeping in the kernel.
 template <class F, int LOGN, int T, int G, int S, bool TERN = false, bool KSC = false>

@@ -766,9 +766,11 @@ void monomial_ntt(const Ntt<F> &ntt, typename F::T c, uint32_t deg, typename F::
 // TernaryBlindRotationKey::blind_rotate (fhe_core/src/blind_rotation/rlwe/ternary.rs:26-119): the
 // LUT rotated by an NTT product with X^-b; per step with a_i != 0 the evaluation key
 // RGSW(s_i == 1) + RGSW(s_i == -1) * NTT(-X^-a_i) (lattice/src/rgsw.rs:321-338) multiplies
-// E = (X^a_i - 1) * ACC, computed through the NTT, and ACC += the product. The fields this path
-// accepts keep canonical words, so the reference's representation-level operations are the
-// canonical ones.
+// E = (X^a_i - 1) * ACC and ACC += the product. The fields this path accepts keep canonical words,
+// so the reference's representation-level operations are the canonical ones. E is the product
+// the reference's comment names (ternary.rs:91), formed here through the transform of the monomial
+// X^a_i; the reference's code places +-1 at index a_i of the NTT-domain vector without transforming
+// it (:93-100), which depends on concrete-ntt's slot order and is not that product.
 template <class F>
 void blind_rotate_ternary(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T *lut_in,
                           uint32_t steps, typename F::T *acc_a, typename F::T *acc_b) {
