@@ -5,7 +5,7 @@
  * Encryptor / Decryptor (tfhe/src/lib.rs:1-13, tfhe/src/bfhe/evaluate.rs), the lattice crate's
  * RLWE x RGSW external product (lattice/src/rlwe.rs:573-596) and the algebra crate's NTT-table trait
  * (algebra/src/transformation/mod.rs:20-96). A Rust binding (hb-gpu-sys) declares these functions
- * verbatim in an `extern "C"` block; see INTEGRATION.md.
+ * verbatim in an `extern "C"` block.
  *
  * Conventions
  *  - Every function returns an int status: HB_OK (0) or a negative HB_ERR_* code. After an error,
