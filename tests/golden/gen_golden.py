@@ -7,8 +7,10 @@ _TERNARY_128_BITS presets, and CUSTOM_TERNARY_128_BITS with a ternary LWE key) w
 records:
 SHA-256 digests of the secret keys, BSK and KSK (the project's seeded key convention); the input
 ciphertexts of the four NAND truth-table rows (encryption seed 0, sample indices 0..7); the oracle's
-NAND outputs. The BabyBear set also records every other gate, a caller-LUT bootstrap, the modulus
-switch of the first NAND input and the blind-rotation accumulator after 1, 2 and 10 steps.
+NAND outputs and their decryption noise; the modulus switch of the first row's combined input
+c0 + c1 (ms0) and the NAND blind-rotation accumulator of that input, [a | b] canonical, after 1, 2
+and 10 steps and after all n steps (acc<n>: the RLWE that enters b[0] += Q/8 and the key switch).
+The BabyBear set also records every other gate and a caller-LUT bootstrap.
 The reference ships no golden vectors (its tests draw from OS entropy), so these files pin the
 oracle and the GPU path against each other and against regressions.
 """
@@ -45,6 +47,13 @@ def main():
         out[f"{name}/c0"] = c0
         out[f"{name}/c1"] = c1
         out[f"{name}/nand"] = O.gate(k, "nand", c0, c1)
+        out[f"{name}/nand_noise"] = O.decrypt(p, k.lwe_sk, out[f"{name}/nand"])[1]
+        q = O.MODULUS[p.field_id]
+        s = np.array([(int(a) + int(b)) % q for a, b in zip(c0[0], c1[0])], O.dtype_of(p.field_id))
+        out[f"{name}/ms0"] = O.modswitch(p, s)
+        nl = O.lut_poly(p.field_id, "nand", p.ring_dim)
+        for steps in (1, 2, 10, p.lwe_dim):
+            out[f"{name}/acc{steps}"] = O.blind_rotate(k, s, nl, steps)
         if pid == O.PRESET_BABYBEAR:
             c2 = O.encrypt(p, k.lwe_sk, 0, 8, np.array([1, 0, 1, 0], np.uint8))
             out[f"{name}/c2"] = c2
@@ -57,12 +66,6 @@ def main():
                                                        dtype=np.uint64)).astype(np.uint32)
             out[f"{name}/lut"] = lut
             out[f"{name}/bootstrap_lut"] = O.bootstrap_lut(k, c0, lut)
-            s = (c0[0].astype(np.uint64) + c1[0].astype(np.uint64)) % O.MODULUS[p.field_id]
-            s = s.astype(np.uint32)
-            out[f"{name}/ms0"] = O.modswitch(p, s)
-            nl = O.lut_poly(p.field_id, "nand", p.ring_dim)
-            for steps in (1, 2, 10):
-                out[f"{name}/acc{steps}"] = O.blind_rotate(k, s, nl, steps)
     np.savez_compressed(os.path.join(HERE, "golden_seed0.npz"), **out)
     print("wrote", os.path.join(HERE, "golden_seed0.npz"), len(out), "arrays")
 

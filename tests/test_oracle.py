@@ -102,7 +102,16 @@ def test_golden_fixtures_reproduce(oracle, oracle_keys):
             assert (out == g[f"{name}/nand"]).all()
         m, noise = oracle.decrypt(k.p, k.lwe_sk, g[f"{name}/nand"])
         assert (m == [1, 1, 1, 0]).all()
+        assert (noise == g[f"{name}/nand_noise"]).all()
         assert (noise < oracle.MODULUS[k.p.field_id] // 16).all()
+        # the first row's combined input through the modulus switch and the blind rotation
+        q = oracle.MODULUS[k.p.field_id]
+        c0, c1 = g[f"{name}/c0"][0], g[f"{name}/c1"][0]
+        s = np.array([(int(a) + int(b)) % q for a, b in zip(c0, c1)], c0.dtype)
+        assert (oracle.modswitch(k.p, s) == g[f"{name}/ms0"]).all()
+        lut = oracle.lut_poly(k.p.field_id, "nand", k.p.ring_dim)
+        for steps in (1, 2, 10, k.p.lwe_dim):
+            assert (oracle.blind_rotate(k, s, lut, steps) == g[f"{name}/acc{steps}"]).all(), steps
 
 
 @pytest.mark.parametrize("set_id", [3, 4, 100])
