@@ -10,6 +10,9 @@ accumulator LUT * X^-b (fhe_core/src/blind_rotation/rlwe/binary.rs:40-64), E = (
 (algebra/src/polynomial/univariate/native_polynomial.rs:340-348), the RLWE x RGSW product
 (lattice/src/rlwe.rs:573-596) and ACC += E (:287-290); for a ternary LWE key the evaluation key
 RGSW(s = 1) + RGSW(s = -1) * (-X^-a) (fhe_core/src/blind_rotation/rlwe/ternary.rs:78-89).
+From the accumulator after all n steps it also recomputes b[0] += Q/8 (tfhe/src/bfhe/evaluate.rs:52),
+the RLWE key switch in n'-word chunks (fhe_core/src/key_switch/rlwe.rs:115-137,250-286) and the
+sample extraction (lattice/src/rlwe.rs:393-402), and gets the committed NAND output.
 
 The arithmetic here is plain arithmetic mod Q. The reference's Goldilocks words may sit in
 [Q, 2^64), where its negation is not the true one (algebra/src/modulus/goldilocks/ops.rs:69-73) and
@@ -112,6 +115,33 @@ def blind_rotate(p, bsk, lwe_sk_ternary, ms, lut, steps, q):
     return np.concatenate([acc_a, acc_b])
 
 
+def key_switch(p, ksk, acc, q):
+    """LWE of dimension n from the accumulator [a | b] (canonical) under the key-switching key
+    ksk[c][j][a|b][n'], n' = next_pow2(n), one gadget RLWE per n'-word chunk of the ring key."""
+    n_ring, n = p.ring_dim, p.lwe_dim
+    m = 1 << (n - 1).bit_length()
+    chunks = n_ring // m
+    a = [int(x) for x in acc[:n_ring]]
+    b0 = (int(acc[n_ring]) + (q >> 3)) % q  # evaluate.rs:52
+    if m != n_ring:  # rlwe.rs:123-131: negate a[0], reverse the rest; then the same per chunk
+        a = [(q - a[0]) % q] + a[1:][::-1]
+        for c in range(chunks):
+            ch = a[c * m:(c + 1) * m]
+            a[c * m:(c + 1) * m] = [(q - ch[0]) % q] + ch[1:][::-1]
+    ksk = ksk.reshape(chunks, p.ks_len, 2, m)
+    pairs_a, pairs_b = [], []
+    for c in range(chunks):
+        # sub_assign_gadget_rlwe_mul_polynomial_inplace_fast (lattice/src/rlwe.rs:1147-1166):
+        # the digits of -a, products added
+        ds = digits([(q - x) % q for x in a[c * m:(c + 1) * m]], p.ks_bits, p.ks_len)
+        pairs_a += [(ds[j], ksk[c, j, 0]) for j in range(p.ks_len)]
+        pairs_b += [(ds[j], ksk[c, j, 1]) for j in range(p.ks_len)]
+    ia, ib = negacyclic_sum(pairs_a, q, m), negacyclic_sum(pairs_b, q, m)
+    # extract_partial_lwe_locally: a' = [A0, -A(n'-1), ..., -A(n'-n+1)], b' = B0 + b0
+    out = [ia[0]] + [(q - ia[m - k]) % q for k in range(1, n)] + [(ib[0] + b0) % q]
+    return np.array(out, dtype=np.uint64)
+
+
 @pytest.mark.parametrize("set_id", ALL_SETS)
 def test_first_steps_without_ntt(oracle, oracle_keys, set_id):
     g = np.load(GOLDEN)
@@ -139,3 +169,15 @@ def test_modswitch_rounding_edges():
     assert modswitch(np.array([q - 1], dtype=np.uint64), q, two_n)[0] == 0
     # (Q + 1) / 2 lands on N
     assert modswitch(np.array([(q + 1) // 2], dtype=np.uint64), q, two_n)[0] == two_n // 2
+
+
+@pytest.mark.parametrize("set_id", ALL_SETS)
+def test_key_switch_and_extraction_without_ntt(oracle, oracle_keys, set_id):
+    g = np.load(GOLDEN)
+    name = oracle.SET_NAMES[set_id]
+    k = oracle_keys(set_id)
+    p = k.p
+    q = oracle.MODULUS[p.field_id]
+    acc = g[f"{name}/acc{p.lwe_dim}"]
+    out = key_switch(p, k.ksk, acc, q)
+    assert (out == g[f"{name}/nand"][0].astype(np.uint64)).all()
