@@ -154,6 +154,9 @@ def test_first_steps_without_ntt(oracle, oracle_keys, set_id):
     ms = modswitch(s, q, 2 * p.ring_dim)
     assert (ms == g[f"{name}/ms0"]).all()
     lut = oracle.lut_poly(p.field_id, "nand", p.ring_dim)
+    # init_nand_lut (tfhe/src/bfhe/evaluate.rs:267-330): Q/8 on [0, 3N/4), -Q/8 on [3N/4, N)
+    mid = 3 * p.ring_dim // 4
+    assert (lut[:mid] == q >> 3).all() and (lut[mid:] == q - (q >> 3)).all()
     ternary = bool(getattr(p, "lwe_ternary", 0))
     for steps in (1, 2):
         acc = blind_rotate(p, k.bsk, ternary, ms, lut, steps, q)
