@@ -172,19 +172,29 @@ def cpu_reference(params_id, gates_per_step, steps, warmup, threads):
     return gates_per_step / statistics.mean(times), statistics.mean(times), lib
 
 
+def gates_workload(gates, set_name, p):
+    """The workload both arms name: `gates` NAND bootstraps under one parameter set."""
+    return (f"{gates} NAND gate bootstraps, {set_name} (N={p.ring_dim}, n={p.lwe_dim}, "
+            f"B=2^{p.br_bits}, l={p.br_len}, KS 2^{p.ks_bits} x {p.ks_len})")
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
+    from oracle import binding as O
     threads = os.cpu_count() or 1
     gates = 4 * threads  # about a second of work per step on the host's cores
-    steps, warmup = args.steps, max(1, min(args.warmup, 1))
-    value, step_s, _ = cpu_reference(PRESET, gates, steps, warmup, threads)
+    steps, warmup = args.steps, args.warmup
+    value, step_s, _ = cpu_reference(args.preset, gates, steps, warmup, threads)
+    p = O.preset(args.preset)
     line = {
         "metric": METRIC, "value": value, "unit": "bootstraps/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": steps, "warmup": warmup, "ms_per_step": step_s * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64" if p.field_id == O.FIELD_GOLDILOCKS else "u32",
         "data": "synthetic (seed-0 keys, seed-3 uniform input bits)",
-        "config": {"workload": "NAND bootstrap, GOLDILOCKS_BINARY_128_BITS (N=1024, n=728, B=2^8, l=8)",
+        "config": {"workload": gates_workload(args.gates, O.PRESET_NAMES[args.preset], p),
+                   "execution": f"a {gates}-gate sample per step, one gate per host thread",
                    "gates_per_step": gates, "parallelism": "one gate per host thread"},
         "cpu_baseline": {"value": value, "unit": "bootstraps/s", "cores": threads, "kind": "port",
                          "sample": f"{gates} NAND gates per step over {threads} threads (C++ oracle: the "
@@ -649,9 +659,8 @@ def main():
         "dtype": "u64" if ws == 8 else "u32",
         "data": "synthetic (seed-0 keys, seed-3 uniform input bits)",
         "config": {
-            "workload": f"{G} NAND gate bootstraps, {set_name} (N={raw.ring_dim}, n={raw.lwe_dim}, "
-                        f"B=2^{raw.br_bits}, l={raw.br_len}, KS 2^{raw.ks_bits} x {raw.ks_len}), "
-                        "one persistent launch per step",
+            "workload": gates_workload(G, set_name, raw),
+            "execution": "one persistent launch per step",
             "gates_per_gpu": G,
             "parallelism": f"replicas x{world}",
             "l2": f"inputs ({2 * G * width * ws / 1e6:.0f} MB) and BSK ({bsk_bytes / 1e6:.0f} MB) "
@@ -688,7 +697,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = 24 * threads  # several seconds of work on the host's cores
-        v, step_s, _ = cpu_reference(PRESET, sample, 1, 0, threads)
+        v, step_s, _ = cpu_reference(args.preset, sample, 1, 0, threads)
         line["cpu_baseline"] = {"value": v, "unit": "bootstraps/s", "cores": threads, "kind": "port",
                                 "sample": f"{sample} NAND gates over {threads} host threads in {step_s:.1f} s "
                                           "(C++ oracle, keys transformed beforehand as Evaluator::new does)"}
