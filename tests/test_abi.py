@@ -25,3 +25,28 @@ def test_library_exports_every_declared_symbol(hb):
     missing = [n for n in declared() if not hasattr(L, n)]
     assert not missing, missing
     assert sorted(_lib.EXPORTS) == declared()
+
+
+def test_every_entry_point_refuses_null_arguments(hb):
+    """Each function, called with null handles and pointers and zero scalars, returns HB_ERR_INVALID
+    (or, where it returns no status, does nothing) without touching a device."""
+    from hasteboots_b200 import _lib
+    L = _lib.lib()
+    for name in declared():
+        fn = getattr(L, name)
+        args = []
+        for t in fn.argtypes:
+            if t in (ctypes.c_double, ctypes.c_float):
+                args.append(0.0)
+            elif t in (ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t,
+                       ctypes.c_longlong):
+                args.append(0)
+            else:
+                args.append(None)
+        rc = fn(*args)
+        if fn.restype is None:
+            assert rc is None, name
+        elif fn.restype in (ctypes.c_size_t, ctypes.c_uint64):
+            assert rc == 0, name
+        else:
+            assert _lib.ERRORS.get(rc) == "HB_ERR_INVALID", (name, rc)

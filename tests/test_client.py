@@ -102,3 +102,12 @@ def test_parameter_validation(hb):
 def bad_params():
     from hasteboots_b200._lib import HbParams
     return HbParams()
+
+
+def test_empty_batches(hb):
+    # zero ciphertexts in, zero out (host encryption and decryption)
+    sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(0), 0)
+    c = sk.encrypt(np.zeros(0, np.uint8))
+    assert c.shape == (0, sk.params.raw.lwe_dim + 1)
+    bits, noise = sk.decrypt_with_noise(c)
+    assert bits.shape == (0,) and noise.shape == (0,)
