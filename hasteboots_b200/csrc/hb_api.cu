@@ -496,7 +496,7 @@ int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t strea
 }
 
 template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
-int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain) {
+int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain, void *trace) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   DevTables *tb;
@@ -517,6 +517,7 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
   if (e != cudaSuccess) return cuda_fail(ctx, e, "job table upload");
   hb::BootParams<W> prm{};
   boot_params(prm, ctx, keys, tb);
+  prm.trace = (W *)trace;
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
@@ -576,7 +577,8 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
 template <class F>
 constexpr int field_of() { return F::FIELD_ID; }
 
-int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain) {
+// trace: the accumulator trace of a one-gate launch (the latency form records it), or null.
+int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain, void *trace = nullptr) {
   if (keys->p.ring_dim != 1024)
     return fail(ctx, HB_ERR_UNSUPPORTED, "bootstrapping is compiled for N = 1024");
   uint64_t gates = 0;
@@ -584,9 +586,11 @@ int run_jobs(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool plain)
   const int G = plain ? 1 : launch_gates_per_cta(ctx, keys, gates), T = keys->threads_per_gate,
             fld = keys->p.field_id;
   const bool tern = keys->p.lwe_ternary != 0, ksc = ks_dim(keys->p) < keys->p.ring_dim;
+  if (trace && (plain || G != 1 || tern || gates != 1))
+    return fail(ctx, HB_ERR_UNSUPPORTED, "accumulator traces are recorded for one gate under a binary LWE key");
 #define HB_CASE(FLD, TT, GG, TN, KC)                                             \
   if (fld == field_of<FLD>() && T == TT && G == GG && tern == TN && ksc == KC) \
-    return launch_boot<FLD, 10, TT, GG, TN, KC>(ctx, keys, jobs, plain);
+    return launch_boot<FLD, 10, TT, GG, TN, KC>(ctx, keys, jobs, plain, trace);
   HB_BOOT_VARIANTS(HB_CASE)
 #undef HB_CASE
   return fail(ctx, HB_ERR_UNSUPPORTED, "no compiled kernel with %d threads per gate and %d gates per CTA", T, G);
@@ -960,6 +964,36 @@ int hb_bootstrap_lut(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut,
   rc = run_jobs(ctx, keys, jobs, false);
   if (rc) return rc;
   cudaError_t e = cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+  return check_status(ctx);
+}
+
+int hb_bootstrap_trace(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut, void *out,
+                       void *acc_trace) {
+  if (!ctx || !keys || !c || !lut || !out || !acc_trace) return HB_ERR_INVALID;
+  if (keys->p.lwe_ternary)
+    return fail(ctx, HB_ERR_UNSUPPORTED, "accumulator traces are recorded under binary LWE keys");
+  cudaSetDevice(ctx->device);
+  const hb_params &p = keys->p;
+  const size_t ws = word_size(p), bytes = (p.lwe_dim + 1) * ws, lbytes = p.ring_dim * ws;
+  const size_t tbytes = (size_t)p.lwe_dim * 2 * p.ring_dim * ws;
+  int rc = scratch(ctx, ctx->io, 2 * bytes + lbytes + tbytes);
+  if (rc) return rc;
+  // every part starts at a multiple of the word size
+  char *din = (char *)ctx->io.ptr, *dout = din + bytes, *dlut = dout + bytes, *dtrace = dlut + lbytes;
+  cudaMemcpyAsync(din, c, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(dlut, lut, lbytes, cudaMemcpyHostToDevice, ctx->stream);
+  GateJob j{};
+  j.in0 = din;
+  j.out = dout;
+  j.lut = dlut;
+  j.s0 = 1;
+  j.count = 1;
+  std::vector<GateJob> jobs{j};
+  rc = run_jobs(ctx, keys, jobs, false, dtrace);
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(acc_trace, dtrace, tbytes, cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
   return check_status(ctx);
 }

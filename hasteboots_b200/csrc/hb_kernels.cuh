@@ -415,6 +415,8 @@ struct BootParams {
   int *status;
   long long budget;
   int withhold;  // test hook: issue no key-chunk copy, so the first wait runs out (bounded)
+  W *trace;      // bootstrap_dp_kernel with one gate: the accumulator after every blind-rotation
+                 // step, [n][a | b][N] canonical words; null records nothing
 };
 
 // Shared memory needed by bootstrap_kernel: twiddles (2N words), S key-chunk stages (2N words
@@ -1056,10 +1058,14 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         NW::inverse(f, wbuf, ping_w, s_itw_w, tw, wsync);
         if (!ks) {
           W *y = half == 0 ? acc_a : acc_b;
+          // the accumulator trace of vfhe's bootstrap (vfhe/src/bfhe/evaluate.rs:47-141), written
+          // by one CTA of the cluster (every CTA forms the same words)
+          W *tr = p.trace != nullptr && rank == 0 ? p.trace + ((size_t)ph * 2 + half) * N : nullptr;
 #pragma unroll
           for (int vw = 0; vw < VW; ++vw) {
             const int k = NW::natural_pos(tw, vw);
             y[k] = F::add(y[k], F::canon(f[vw]));  // RLWE::add_assign_element_wise
+            if (tr) tr[k] = F::canon(y[k]);
           }
         } else if (rank == 0) {
           // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402); b' = acc.b[0] + Q/8 + B0; with

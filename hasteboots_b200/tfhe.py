@@ -324,6 +324,20 @@ class Evaluator:
                                      _ptr(out), len(c)), "bootstrap", self.ctx.handle)
         return out
 
+    def bootstrap_with_trace(self, c, lut):
+        """bootstrap of one ciphertext plus the accumulator after every blind-rotation step (the
+        AccTrace of vfhe's bootstrap, vfhe/src/bfhe/evaluate.rs:47-141): returns (out [n + 1],
+        trace [n, 2N] with a in [:, :N] and b in [:, N:])."""
+        dt = self.params.dtype
+        n, N = self.params.lwe_dimension(), self.params.ring_dimension()
+        c = np.ascontiguousarray(c, dt).reshape(n + 1)
+        lut = np.ascontiguousarray(lut, dt)
+        out = np.zeros(n + 1, dt)
+        trace = np.zeros((n, 2 * N), dt)
+        check(lib().hb_bootstrap_trace(self.ctx.handle, self.keys.handle, _ptr(c), _ptr(lut),
+                                       _ptr(out), _ptr(trace)), "bootstrap_with_trace", self.ctx.handle)
+        return out, trace
+
 
 # ------------------------------------------------------------------------------------------------
 # Autotuning and mixed-set batches

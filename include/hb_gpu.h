@@ -170,6 +170,14 @@ int hb_gate_device_plain(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, c
  * one LUT polynomial of N words. Host buffers. */
 int hb_bootstrap_lut(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut, void *out,
                      size_t count);
+/* EvaluationKey::bootstrap(c, lut) of one ciphertext that also returns the blind-rotation
+ * accumulator after every step, the AccTrace that vfhe's bootstrap records for its proof
+ * (vfhe/src/bfhe/evaluate.rs:47-141): acc_trace receives n x 2N canonical words, step i's
+ * accumulator a at [i][0, N) and b at [i][N, 2N), before b[0] += Q/8 and the key switch. Steps
+ * with a zero rotation leave the accumulator as it was. Host buffers; binary LWE keys
+ * (HB_ERR_UNSUPPORTED for a ternary one). */
+int hb_bootstrap_trace(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut, void *out,
+                       void *acc_trace);
 
 /* ---- NTT table trait and external product (device slices) ---------------------------------- */
 
