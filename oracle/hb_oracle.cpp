@@ -186,6 +186,24 @@ struct Ntt {
   std::vector<T> zeta, izeta;  // zeta[k] = psi^brv(k), izeta[k] = psi^-brv(k), k in [1, n)
   T n_inv = 0;
   bool ok = false;
+  // 32-bit fields: Shoup's precomputed quotients w' = floor(w 2^32 / P) of every constant factor
+  // (V. Shoup's NTL MulModPrecon; D. Harvey, "Faster arithmetic for number-theoretic transforms",
+  // J. Symb. Comput. 60, 2014): for a < 2^32 and w < P < 2^31, a w - floor(a w' / 2^32) P lies in
+  // [0, 2P), so one conditional subtraction gives the canonical a w mod P.
+  std::vector<uint32_t> zeta_q, izeta_q;
+  uint32_t n_inv_q = 0;
+
+  static uint32_t quotient(T w) { return (uint32_t)(((uint64_t)w << 32) / F::P); }
+  static T mul_q(T a, T w, uint32_t wq) {
+    if constexpr (sizeof(T) == 4) {
+      const uint32_t q = (uint32_t)(((uint64_t)a * wq) >> 32);
+      const uint32_t r = (uint32_t)a * (uint32_t)w - q * (uint32_t)F::P;
+      return (T)(r >= F::P ? r - F::P : r);
+    } else {
+      (void)wq;
+      return F::mul(a, w);
+    }
+  }
 
   explicit Ntt(uint32_t log_n) : logn(log_n), n(1u << log_n) {
     uint64_t order = (uint64_t)F::P - 1;
@@ -215,6 +233,15 @@ struct Ntt {
       izeta[k] = ipw[bit_reverse(k, logn)];
     }
     n_inv = finv<F>((T)n);
+    if constexpr (sizeof(T) == 4) {
+      zeta_q.assign(n, 0);
+      izeta_q.assign(n, 0);
+      for (uint32_t k = 1; k < n; ++k) {
+        zeta_q[k] = quotient(zeta[k]);
+        izeta_q[k] = quotient(izeta[k]);
+      }
+      n_inv_q = quotient(n_inv);
+    }
     ok = true;
   }
 
@@ -224,12 +251,16 @@ struct Ntt {
     uint32_t k = 1;
     for (uint32_t len = n >> 1; len >= 1; len >>= 1)
       for (uint32_t start = 0; start < n; start += 2 * len) {
-        const T w = zeta[k++];
-        for (uint32_t j = start; j < start + len; ++j) {
-          const T t = F::mul(a[j + len], w);
-          const T u = a[j];
-          a[j] = F::add_cc(u, t);
-          a[j + len] = F::sub_cc(u, t);
+        const T w = zeta[k];
+        const uint32_t wq = sizeof(T) == 4 ? zeta_q[k] : 0;
+        ++k;
+        T *__restrict lo = a + start;  // the two halves of a block never overlap
+        T *__restrict hi = lo + len;
+        for (uint32_t j = 0; j < len; ++j) {
+          const T t = mul_q(hi[j], w, wq);
+          const T u = lo[j];
+          lo[j] = F::add_cc(u, t);
+          hi[j] = F::sub_cc(u, t);
         }
       }
   }
@@ -240,14 +271,17 @@ struct Ntt {
       const uint32_t blocks = n / (2 * len);
       for (uint32_t blk = 0; blk < blocks; ++blk) {
         const T w = izeta[blocks + blk];
-        for (uint32_t j = 2 * len * blk; j < 2 * len * blk + len; ++j) {
-          const T u = a[j], v = a[j + len];
-          a[j] = F::add_cc(u, v);
-          a[j + len] = F::mul(F::sub_cc(u, v), w);
+        const uint32_t wq = sizeof(T) == 4 ? izeta_q[blocks + blk] : 0;
+        T *__restrict lo = a + 2 * len * blk;
+        T *__restrict hi = lo + len;
+        for (uint32_t j = 0; j < len; ++j) {
+          const T u = lo[j], v = hi[j];
+          lo[j] = F::add_cc(u, v);
+          hi[j] = mul_q(F::sub_cc(u, v), w, wq);
         }
       }
     }
-    for (uint32_t i = 0; i < n; ++i) a[i] = F::mul(a[i], n_inv);
+    for (uint32_t i = 0; i < n; ++i) a[i] = mul_q(a[i], n_inv, n_inv_q);
   }
 };
 
