@@ -70,6 +70,19 @@ struct Gold {
     return s - (P & mask((s < a) | (s >= P)));
   }
   static T sub_cc(T a, T b) { return a - b + (P & mask(a < b)); }
+  // Lazy operations for the transforms: any word in [0, 2^64) stands for its residue. A carry out
+  // of a + b is worth 2^64 = EPS (mod P); after one carry the sum is at most 2^64 - 2, so adding
+  // EPS carries at most once more, and then the word is below 2^33. A borrow is worth -EPS the
+  // same way; a second borrow leaves at least 2^64 - 2 EPS, so the third subtraction cannot wrap.
+  static T add_lz(T a, T b) {
+    const T s = a + b, e = EPS & mask(s < a), s2 = s + e;
+    return s2 + (EPS & mask(s2 < e));
+  }
+  static T sub_lz(T a, T b) {
+    const T d = a - b, e = EPS & mask(a < b);
+    return d - e - (EPS & mask(d < e));
+  }
+  static T mul_lz(T a, T b) { return fold128((u128)a * b); }
   // Sum of products reduced once: fold128 values (< 2^64) added in 128 bits.
   typedef u128 Acc;
   static void acc_mac(Acc &acc, T a, T b) { acc += fold128((u128)a * b); }
@@ -204,6 +217,17 @@ struct Ntt {
       return F::mul(a, w);
     }
   }
+  // Butterfly operations: Goldilocks words stay lazy inside a transform (canonical at its end),
+  // the 32-bit fields' words stay canonical.
+  static T bf_add(T a, T b) {
+    if constexpr (sizeof(T) == 8) return F::add_lz(a, b); else return F::add_cc(a, b);
+  }
+  static T bf_sub(T a, T b) {
+    if constexpr (sizeof(T) == 8) return F::sub_lz(a, b); else return F::sub_cc(a, b);
+  }
+  static T bf_mul(T a, T w, uint32_t wq) {
+    if constexpr (sizeof(T) == 8) return F::mul_lz(a, w); else return mul_q(a, w, wq);
+  }
 
   explicit Ntt(uint32_t log_n) : logn(log_n), n(1u << log_n) {
     uint64_t order = (uint64_t)F::P - 1;
@@ -257,12 +281,14 @@ struct Ntt {
         T *__restrict lo = a + start;  // the two halves of a block never overlap
         T *__restrict hi = lo + len;
         for (uint32_t j = 0; j < len; ++j) {
-          const T t = mul_q(hi[j], w, wq);
+          const T t = bf_mul(hi[j], w, wq);
           const T u = lo[j];
-          lo[j] = F::add_cc(u, t);
-          hi[j] = F::sub_cc(u, t);
+          lo[j] = bf_add(u, t);
+          hi[j] = bf_sub(u, t);
         }
       }
+    if constexpr (sizeof(T) == 8)
+      for (uint32_t i = 0; i < n; ++i) a[i] = F::canon(a[i]);
   }
   // AbstractNTT::inverse_transform_slice (algebra/src/transformation/mod.rs:95): inverse + normalize
   void inverse(T *a) const {
@@ -276,8 +302,8 @@ struct Ntt {
         T *__restrict hi = lo + len;
         for (uint32_t j = 0; j < len; ++j) {
           const T u = lo[j], v = hi[j];
-          lo[j] = F::add_cc(u, v);
-          hi[j] = mul_q(F::sub_cc(u, v), w, wq);
+          lo[j] = bf_add(u, v);
+          hi[j] = bf_mul(bf_sub(u, v), w, wq);
         }
       }
     }
