@@ -95,6 +95,7 @@ def lib():
         L.orc_bootstrap_lut.argtypes = [P, vp, vp, vp, vp, vp, sz, i32]
         L.orc_modswitch.argtypes = [P, vp, vp]
         L.orc_blind_rotate.argtypes = [P, vp, vp, vp, ctypes.c_uint32, vp]
+        L.orc_blind_rotate_trace.argtypes = [P, vp, vp, vp, vp]
         L.orc_ntt_roundtrip.argtypes = [i32, ctypes.c_uint32, vp, vp]
         L.orc_negacyclic_mul.argtypes = [i32, ctypes.c_uint32, vp, vp, vp, i32]
         L.orc_external_product.argtypes = [i32, ctypes.c_uint32, ctypes.c_uint32,
@@ -230,6 +231,18 @@ def blind_rotate(keys, c, lut, steps):
     out = np.zeros(2 * p.ring_dim, dt)
     _check(lib().orc_blind_rotate(ctypes.byref(p), _ptr(keys.bsk), _ptr(c), _ptr(lut), steps,
                                   _ptr(out)), "blind_rotate")
+    return out
+
+
+def blind_rotate_trace(keys, c, lut):
+    """The accumulator after every blind-rotation step: [n, 2N] (a then b, canonical)."""
+    p = keys.p
+    dt = dtype_of(p.field_id)
+    c = np.ascontiguousarray(c, dtype=dt)
+    lut = np.ascontiguousarray(lut, dtype=dt)
+    out = np.zeros((p.lwe_dim, 2 * p.ring_dim), dt)
+    _check(lib().orc_blind_rotate_trace(ctypes.byref(p), _ptr(keys.bsk), _ptr(c), _ptr(lut),
+                                        _ptr(out)), "blind_rotate_trace")
     return out
 
 

@@ -766,11 +766,23 @@ void external_product(const Ntt<F> &ntt, uint32_t bits, uint32_t L, const typena
   std::copy(mb, mb + N, eb);
 }
 
+// One row of an accumulator trace: [a | b] canonical (the rows of AccTrace, trace/src/acc_trace.rs).
+template <class F>
+void trace_row(const typename F::T *acc_a, const typename F::T *acc_b, uint32_t N, typename F::T *row) {
+  for (uint32_t k = 0; k < N; ++k) {
+    row[k] = F::canon(acc_a[k]);
+    row[N + k] = F::canon(acc_b[k]);
+  }
+}
+
 // BinaryBlindRotationKey::blind_rotate (fhe_core/src/blind_rotation/rlwe/binary.rs:28-104).
-// acc_a/acc_b hold the reference's representation of the accumulator.
+// acc_a/acc_b hold the reference's representation of the accumulator. With `trace`, the accumulator
+// after every step i goes to trace[i] (blind_rotate_w_trace, binary.rs:106-205, which does not skip
+// a_i = 0; such a step leaves the accumulator unchanged).
 template <class F>
 void blind_rotate(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T *lut_in,
-                  uint32_t steps, typename F::T *acc_a, typename F::T *acc_b) {
+                  uint32_t steps, typename F::T *acc_a, typename F::T *acc_b,
+                  typename F::T *trace = nullptr) {
   using T = typename F::T;
   const Dims &d = ek.d;
   const uint32_t N = d.N;
@@ -796,16 +808,18 @@ void blind_rotate(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T 
   std::vector<T> ea(N), eb(N);
   const size_t entry = (size_t)2 * d.len * 2 * N;
   for (uint32_t i = 0; i < d.n && i < steps; ++i) {
-    uint32_t ai = ms[i];
-    if (ai == 0) continue;  // binary.rs:70
-    monomial_sub_one<F>(acc_a, ea.data(), N, ai);
-    monomial_sub_one<F>(acc_b, eb.data(), N, ai);
-    external_product<F>(ntt, d.bits, d.len, ek.bsk_ntt.data() + i * entry, ea.data(), eb.data());
-    // RLWE::add_assign_element_wise (lattice/src/rlwe.rs:287-290)
-    for (uint32_t k = 0; k < N; ++k) {
-      acc_a[k] = F::add_ref(acc_a[k], ea[k]);
-      acc_b[k] = F::add_ref(acc_b[k], eb[k]);
+    const uint32_t ai = ms[i];
+    if (ai != 0) {  // binary.rs:70
+      monomial_sub_one<F>(acc_a, ea.data(), N, ai);
+      monomial_sub_one<F>(acc_b, eb.data(), N, ai);
+      external_product<F>(ntt, d.bits, d.len, ek.bsk_ntt.data() + i * entry, ea.data(), eb.data());
+      // RLWE::add_assign_element_wise (lattice/src/rlwe.rs:287-290)
+      for (uint32_t k = 0; k < N; ++k) {
+        acc_a[k] = F::add_ref(acc_a[k], ea[k]);
+        acc_b[k] = F::add_ref(acc_b[k], eb[k]);
+      }
     }
+    if (trace) trace_row<F>(acc_a, acc_b, N, trace + (size_t)i * 2 * N);
   }
 }
 
@@ -833,7 +847,8 @@ void monomial_ntt(const Ntt<F> &ntt, typename F::T c, uint32_t deg, typename F::
 // it (:93-100), which depends on concrete-ntt's slot order and is not that product.
 template <class F>
 void blind_rotate_ternary(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T *lut_in,
-                          uint32_t steps, typename F::T *acc_a, typename F::T *acc_b) {
+                          uint32_t steps, typename F::T *acc_a, typename F::T *acc_b,
+                          typename F::T *trace = nullptr) {
   using T = typename F::T;
   const Dims &d = ek.d;
   const uint32_t N = d.N;
@@ -852,7 +867,10 @@ void blind_rotate_ternary(const EvalKey<F> &ek, const uint32_t *ms, const typena
   std::vector<T> evk(rgsw), ea(N), eb(N);
   for (uint32_t i = 0; i < d.n && i < steps; ++i) {
     const uint32_t ai = ms[i];
-    if (ai == 0) continue;  // ternary.rs:73
+    if (ai == 0) {  // ternary.rs:73
+      if (trace) trace_row<F>(acc_a, acc_b, N, trace + (size_t)i * 2 * N);
+      continue;
+    }
     // evaluation_key = RGSW_0 + RGSW_1 * NTT(-X^(2N - a_i)) (ternary.rs:78-89)
     monomial_ntt<F>(ntt, (T)(F::P - 1), 2 * N - ai, mono.data());
     const T *k0 = ek.bsk_ntt.data() + (size_t)i * 2 * rgsw;
@@ -874,6 +892,7 @@ void blind_rotate_ternary(const EvalKey<F> &ek, const uint32_t *ms, const typena
       acc_a[k] = F::add(acc_a[k], ea[k]);
       acc_b[k] = F::add(acc_b[k], eb[k]);
     }
+    if (trace) trace_row<F>(acc_a, acc_b, N, trace + (size_t)i * 2 * N);
   }
 }
 
@@ -1220,8 +1239,9 @@ int orc_modswitch(const orc_params *p, const void *c, uint32_t *out) {
   return 0;
 }
 
-int orc_blind_rotate(const orc_params *p, const void *bsk, const void *c, const void *lut,
-                     uint32_t steps, void *acc_out) {
+// The accumulator after `steps` steps (acc_out: 2N words), and with `trace` every step's row.
+static int blind_rotate_probe(const orc_params *p, const void *bsk, const void *c, const void *lut,
+                       uint32_t steps, void *acc_out, void *trace) {
   Dims d;
   if (!dims_of(p, d)) return -1;
   ORC_DISPATCH(p, {
@@ -1240,12 +1260,24 @@ int orc_blind_rotate(const orc_params *p, const void *bsk, const void *c, const 
     modswitch<F>(d, (const T *)c, ms.data());
     T *acc = (T *)acc_out;
     if (d.pairs == 2)
-      blind_rotate_ternary<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N);
+      blind_rotate_ternary<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N, (T *)trace);
     else
-      blind_rotate<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N);
+      blind_rotate<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N, (T *)trace);
     for (uint32_t k = 0; k < 2 * d.N; ++k) acc[k] = F::canon(acc[k]);
   });
   return 0;
+}
+
+int orc_blind_rotate(const orc_params *p, const void *bsk, const void *c, const void *lut,
+                     uint32_t steps, void *acc_out) {
+  return blind_rotate_probe(p, bsk, c, lut, steps, acc_out, nullptr);
+}
+
+int orc_blind_rotate_trace(const orc_params *p, const void *bsk, const void *c, const void *lut,
+                           void *trace_out) {
+  if (!p || !trace_out) return -1;
+  std::vector<uint64_t> acc(2 * (size_t)p->ring_dim);  // room for either word size
+  return blind_rotate_probe(p, bsk, c, lut, p->lwe_dim, acc.data(), trace_out);
 }
 
 int orc_ntt_roundtrip(int field_id, uint32_t log_n, const void *in, void *out) {

@@ -155,3 +155,25 @@ def test_cbd_error_polynomials(oracle):
             errs.append(e)
     e = np.concatenate(errs)
     assert e.max() <= 13 and e.min() == 0 and np.count_nonzero(e) > len(e) // 2
+
+
+def test_blind_rotation_trace_rows(oracle, oracle_keys):
+    # one pass over all n steps gives the per-step probes' accumulators (golden rows 1, 2, 10, n),
+    # and a step whose rotation is zero repeats the previous row; binary and ternary LWE keys
+    g = np.load(GOLDEN)
+    for pid in (0, 100):
+        name = oracle.SET_NAMES[pid]
+        k = oracle_keys(pid)
+        q = oracle.MODULUS[k.p.field_id]
+        c0, c1 = g[f"{name}/c0"][0], g[f"{name}/c1"][0]
+        s = np.array([(int(a) + int(b)) % q for a, b in zip(c0, c1)], c0.dtype)
+        lut = oracle.lut_poly(k.p.field_id, "nand", k.p.ring_dim)
+        rows = oracle.blind_rotate_trace(k, s, lut)
+        n = k.p.lwe_dim
+        assert rows.shape == (n, 2 * k.p.ring_dim)
+        for steps in (1, 2, 10, n):
+            assert (rows[steps - 1] == g[f"{name}/acc{steps}"]).all(), (pid, steps)
+        ms = g[f"{name}/ms0"]
+        for i in range(1, n):
+            if ms[i] == 0:
+                assert (rows[i] == rows[i - 1]).all(), (pid, i)
