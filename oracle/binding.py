@@ -1,7 +1,7 @@
 """ctypes binding of the CPU oracle (oracle/libhb_oracle.so) -- TEST INFRASTRUCTURE ONLY.
 
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, as the
-checker. It restates the reference's TFHE gate-bootstrapping path on the CPU; see hb_oracle.h for
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg and reference arm
+(--impl reference) use this module; tests and smoke() use it as the checker. It restates the reference's TFHE gate-bootstrapping path on the CPU; see hb_oracle.h for
 the reference files it follows and its parity status.
 """
 

@@ -6,8 +6,9 @@
  * RLWE/RGSW external product, algebra Goldilocks/BabyBear/DefaultFieldU32 arithmetic and unsigned
  * gadget decomposition).
  *
- * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load this library,
- * and only as the checker. The product (hasteboots_b200/, libhb_gpu.so) never links it.
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg and reference arm
+ * (--impl reference, the timed CPU restatement) may load this library, tests and smoke() only as
+ * the checker. The product (hasteboots_b200/, libhb_gpu.so) never links it.
  *
  * Parity status: the reference (pure Rust, NTT in the un-vendored `concrete-ntt` git
  * dependency, branch `dev`, no pinned commit) cannot be built or run in this environment
