@@ -1,7 +1,8 @@
 // hb_oracle.cpp -- TEST INFRASTRUCTURE ONLY (see hb_oracle.h for scope and parity status).
 //
 // CPU restatement of the reference's TFHE NAND/gate bootstrapping path. Every function cites
-// the reference file:line it follows. Arithmetic inside transforms is canonical; where the
+// the reference file:line it follows. Transforms are exact over Z/QZ with canonical inputs and
+// outputs (Goldilocks words may leave [0, Q) between butterflies, never between calls); where the
 // reference's own code fixes a (possibly non-canonical) Goldilocks representation that can leak
 // into results -- accumulator additions and negations -- this file reproduces the reference's
 // exact u64 operations (algebra/src/modulus/goldilocks/ops.rs).
