@@ -1296,24 +1296,35 @@ constexpr size_t kNoAllocStatus = 0;         // int status word
 constexpr size_t kNoAllocJobs = 256;         // three GateJob records
 constexpr size_t kNoAllocData = 1024;        // t0 | t1, count * (n + 1) words each
 
+static_assert(kNoAllocStatus + sizeof(int) <= kNoAllocJobs, "status word overlaps the job table");
+static_assert(kNoAllocJobs + 3 * sizeof(GateJob) <= kNoAllocData, "job table overlaps the ciphertexts");
+
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[256] = {};  // device address of g_noalloc_scratch, per device
 
 // Host code only sees a host-side stand-in named g_noalloc_scratch; the kernels need the device
-// address, looked up once per device with that device current.
+// address, looked up with the context's device current by the first call on each context (kept
+// on the context, so a context created after a device reset never uses a stale address).
 int noalloc_address(hb_ctx *ctx, unsigned char **out) {
-  if (ctx->device < 0 || ctx->device >= 256) return fail(ctx, HB_ERR_INVALID, "device id out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[ctx->device]) {
+  if (!ctx->noalloc_addr) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(no-allocation scratch)");
-    g_noalloc_addr[ctx->device] = p;
+    ctx->noalloc_addr = p;
   }
-  *out = (unsigned char *)g_noalloc_addr[ctx->device];
+  *out = (unsigned char *)ctx->noalloc_addr;
   return HB_OK;
+}
+
+// Gates per CTA of the allocation-free MUX: the keys' variant, or, when that is the one-gate
+// latency variant (which the batched launches here do not use), the smallest compiled G > 1 for
+// the keys' group size.
+int noalloc_gates_per_cta(const hb_keys *keys) {
+  if (keys->gates_per_cta > 1) return keys->gates_per_cta;
+  std::vector<int> v = variants(keys->p, keys->threads_per_gate);
+  return v.empty() ? 0 : *std::min_element(v.begin(), v.end());
 }
 
 template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
@@ -1326,8 +1337,7 @@ int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJo
   prm.jobs = djobs;
   prm.njobs = njobs;
   prm.total_batches = batches;
-  prm.status = dstatus;
-  prm.withhold = 0;
+  prm.status = dstatus;  // withhold keeps the context's test setting (boot_params)
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);
@@ -1340,8 +1350,8 @@ int launch_noalloc(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJo
 }
 
 int noalloc_layer(hb_ctx *ctx, hb_keys *keys, const DevTables *tb, const GateJob *djobs, int njobs,
-                  uint32_t batches, int *dstatus) {
-  const int G = keys->gates_per_cta, T = keys->threads_per_gate, fld = keys->p.field_id;
+                  uint32_t batches, int *dstatus, int G) {
+  const int T = keys->threads_per_gate, fld = keys->p.field_id;
   const bool tern = keys->p.lwe_ternary != 0, ksc = ks_dim(keys->p) < keys->p.ring_dim;
 #define HB_CASE(FLD, TT, GG, TN, KC)                                                       \
   if (fld == field_of<FLD>() && T == TT && G == GG && GG > 1 && tern == TN && ksc == KC) \
@@ -1382,7 +1392,8 @@ extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void
 
   // MUX (tfhe/src/bfhe/evaluate.rs:245-262): t0 = and(c0, c1), t1 = and(not c0, c2) in one launch,
   // then out = bootstrap(t0 + t1, or) in a second.
-  const int G = keys->gates_per_cta;
+  const int G = noalloc_gates_per_cta(keys);
+  if (G <= 1) return fail(ctx, HB_ERR_UNSUPPORTED, "no batched kernel compiled for these keys");
   GateJob jobs[3];
   jobs[0] = make_job(P, HB_GATE_AND, p.ring_dim, c0, c1, nullptr, t0, (uint32_t)count);
   jobs[1] = jobs[0];
@@ -1401,14 +1412,17 @@ extern "C" int hb_gate_mux_device_noalloc(hb_ctx *ctx, hb_keys *keys, const void
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(djobs, jobs, sizeof(jobs), cudaMemcpyHostToDevice, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "no-allocation scratch setup");
-  rc = noalloc_layer(ctx, keys, tb, djobs, 2, 2 * per_job, dstatus);
-  if (!rc) rc = noalloc_layer(ctx, keys, tb, djobs + 2, 1, per_job, dstatus);
-  if (rc) return rc;
+  // The second layer reads t0 and t1, so it runs only when the first one finished all its waits.
   int h = 0;
-  e = cudaMemcpyAsync(&h, dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "no-allocation MUX");
-  if (h) return fail(ctx, HB_ERR_TIMEOUT, "a device-side wait exceeded its limit (status %d)", h);
+  for (int layer = 0; layer < 2; ++layer) {
+    rc = layer == 0 ? noalloc_layer(ctx, keys, tb, djobs, 2, 2 * per_job, dstatus, G)
+                    : noalloc_layer(ctx, keys, tb, djobs + 2, 1, per_job, dstatus, G);
+    if (rc) return rc;
+    e = cudaMemcpyAsync(&h, dstatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "no-allocation MUX");
+    if (h) return fail(ctx, HB_ERR_TIMEOUT, "a device-side wait exceeded its limit (status %d)", h);
+  }
   return HB_OK;
 }
 

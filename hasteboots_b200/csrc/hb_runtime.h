@@ -47,6 +47,9 @@ struct hb_ctx {
   // co-resident latency-form clusters (Goldilocks, T = 64 / 128); -1 unknown. Atomic: the serving
   // loop's worker thread launches on the context too.
   std::atomic<int> dp_clusters[2] = {-1, -1};
+  // device address of the allocation-free MUX's in-library array, looked up by the first such call
+  // on this context (a context made after a device reset looks it up again)
+  void *noalloc_addr = nullptr;
 };
 
 struct hb_keys {

@@ -283,8 +283,9 @@ int hb_serve_stop(hb_server *s);
  * library, which every GPU that loads the library holds until the process exits. count is at most
  * (16 MiB - 1 KiB) / (2 (n + 1) word bytes): 1438 gates for the Goldilocks sets, 2876 for BabyBear,
  * 2045 for DEFAULT_TERNARY, 4087 for CUSTOM_TERNARY; larger counts return HB_ERR_INVALID. The
- * first call on a device looks up the array's device address, so make that call before any stream
- * capture. Every call uses the same array: calls whose work overlaps on the GPU (other streams,
+ * first call on a context looks up the array's device address, so make that call before any stream
+ * capture. A wait that runs out in the first of the two bootstrap layers returns HB_ERR_TIMEOUT
+ * without running the second. Every call uses the same array: calls whose work overlaps on the GPU (other streams,
  * contexts or host threads) race and must be serialised. Device pointers in; returns when `out`
  * holds the result (synchronises the context stream). The keys must have been created (uploaded or
  * generated) on this context. */

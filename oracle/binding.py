@@ -71,14 +71,30 @@ def build():
 
 
 _lib = None
+_lib_path = LIB_PATH
+
+
+def use_native_build():
+    """Before the first lib() call: build the oracle for this host's CPU (-march=native, `make
+    native`) and load that build. Returns a description of the build used; falls back to the
+    portable library when the native build fails."""
+    global _lib_path
+    if _lib is not None:
+        return "portable (loaded before the native build was requested)"
+    try:
+        subprocess.run(["make", "-s", "-C", HERE, "native"], check=True, capture_output=True, timeout=600)
+        _lib_path = os.path.join(HERE, "libhb_oracle_native.so")
+        return "-O3 -march=native, built on this host"
+    except (OSError, subprocess.SubprocessError):
+        return "-O3 portable (the native build failed)"
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
+        if _lib_path == LIB_PATH and not os.path.exists(LIB_PATH):
             build()
-        L = ctypes.CDLL(LIB_PATH)
+        L = ctypes.CDLL(_lib_path)
         vp, sz, u64, i32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int
         P = ctypes.POINTER(OrcParams)
         L.orc_params_preset.argtypes = [i32, P]

@@ -1,6 +1,7 @@
-"""Parity at the full sizes of the measured workloads, through properties that do not need the
-oracle to redo the whole batch: exact NTT round trips on 4096 polynomials, sampled external
-products and sampled gates against the oracle, truth tables and noise bounds on every gate."""
+"""Parity at the full sizes of the measured workloads: exact NTT round trips on 4096 polynomials,
+sampled external products against the oracle, and every output ciphertext of the 16384-gate
+headline batch and of the 64-job mixed-set batch against the oracle's, through the SHA-256 digests
+that tests/golden/gen_digests.py recorded by running the oracle on the same inputs."""
 
 import ctypes
 
@@ -52,58 +53,77 @@ def test_ntt_and_external_product_4096(hb, oracle, ctx, log_n):
     assert (got[sample] == expect).all()
 
 
-def test_16384_goldilocks_nand(hb, oracle, oracle_keys, ctx):
-    """The headline batch: every gate decrypts to NAND with noise below Q/16, sampled gates equal
-    the oracle bit for bit."""
+
+
+def _digests():
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "digests_full.json")
+    return json.load(open(path))
+
+
+def test_16384_goldilocks_nand_every_output(hb, ctx):
+    """The headline batch: every one of the 16384 output ciphertexts equals the oracle's, through the
+    SHA-256 of each 1024-gate slice (tests/golden/gen_digests.py ran the oracle on the same inputs,
+    whose digests are checked first); every gate decrypts to NAND with noise below Q/16."""
+    from hasteboots_b200 import workloads as W
     from hasteboots_b200._lib import check, lib
-    params = hb.Parameters.preset(GOLDILOCKS)
+    ref = _digests()["headline"]
+    params = hb.Parameters.preset(W.HEADLINE_PRESET)
     sk = hb.KeyGen.generate_secret_key(params, 0)
     ev = hb.Evaluator(sk, ctx)
-    count = 16384
-    bits = np.random.default_rng(3).integers(0, 2, (2, count)).astype(np.uint8)
-    c0, c1 = sk.encrypt(bits[0], 0), sk.encrypt(bits[1], 1 << 20)
+    count = W.HEADLINE_GATES
+    bits = W.headline_bits(count)
+    c0, c1 = sk.encrypt(bits[0], W.HEADLINE_INDEX0[0]), sk.encrypt(bits[1], W.HEADLINE_INDEX0[1])
+    assert W.digest(c0) == ref["c0"] and W.digest(c1) == ref["c1"]
     d0, d1, dout = to_dev(c0), to_dev(c1), empty_dev(c0.shape, c0.dtype)
     check(lib().hb_gate_device(ctx.handle, ev.keys.handle, 0, ptr(d0), ptr(d1), None, ptr(dout), count),
           "nand", ctx.handle)
     ctx.synchronize()
     out = from_dev(dout, c0.dtype)
     m, noise = sk.decrypt_with_noise(out)
-    assert (m == 1 - (bits[0] & bits[1])).all()
+    assert (m == W.truth("nand", bits[0], bits[1])).all()
     assert (noise < params.modulus // 16).all()
-    keys = oracle_keys(GOLDILOCKS, 0)
-    for i in (0, 9001, count - 1):
-        ref = oracle.gate(keys, "nand", c0[i:i + 1], c1[i:i + 1])
-        assert (out[i:i + 1] == ref).all(), i
+    got = W.slice_digests(out, ref["slice"])
+    bad = [i for i, (a, b) in enumerate(zip(got, ref["out_slices"])) if a != b]
+    assert len(ref["out_slices"]) == count // ref["slice"] and not bad, f"slices differing: {bad}"
     ev.keys.free()
 
 
-def test_64_mixed_jobs(hb, ctx):
-    """The mixed-set workload: 64 jobs, log-uniform 1-4096 gates, sets drawn from the three presets,
-    in one graph; every gate decrypts to its truth table."""
+def test_64_mixed_jobs_every_output(hb, ctx):
+    """The mixed-set workload: 64 jobs of seven gate kinds, log-uniform 1-4096 gates, sets drawn from
+    the three presets, in one graph; every job's outputs equal the oracle's (SHA-256 per job, inputs
+    checked first) and decrypt to the job's truth table."""
+    from hasteboots_b200 import workloads as W
+    ref = _digests()["mixed"]
     evs = {}
     for pid in (0, 1, 2):
         sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(pid), 0)
         evs[pid] = (sk, hb.Evaluator(sk, ctx))
-    rng = np.random.default_rng(4)
-    jobs, expect = [], []
-    for i in range(64):
-        pid = int(rng.integers(0, 3))
-        count = int(np.clip(np.round(np.exp(rng.uniform(0, np.log(4096)))), 1, 4096))
-        sk, ev = evs[pid]
-        bits = rng.integers(0, 2, (2, count)).astype(np.uint8)
-        c0, c1 = sk.encrypt(bits[0], (i << 24) + 1), sk.encrypt(bits[1], (i << 24) + (1 << 20))
-        out = empty_dev(c0.shape, c0.dtype)
-        jobs.append((ev, "nand", to_dev(c0), to_dev(c1), None, out))
-        expect.append((pid, 1 - (bits[0] & bits[1])))
+    jobs, plan = [], W.mixed_plan()
+    assert len(ref) == len(plan)
+    for job in plan:
+        sk, ev = evs[job.preset]
+        cs = [sk.encrypt(job.bits[k], job.index0(k)) for k in range(job.inputs)]
+        r = ref[str(job.index)]
+        assert (r["preset"], r["gate"], r["count"]) == (job.preset, job.gate, job.count)
+        assert [W.digest(c) for c in cs] == r["inputs"], job.index
+        d = [to_dev(c) for c in cs]
+        out = empty_dev(cs[0].shape, cs[0].dtype)
+        jobs.append((ev, job.gate, d[0], d[1], d[2] if job.inputs == 3 else None, out))
     batch = hb.Batch(ctx, jobs)
     batch.launch()
     ctx.synchronize()
-    for job, (pid, exp) in zip(jobs, expect):
-        sk = evs[pid][0]
-        got = from_dev(job[5], sk.params.dtype)
+    bad = []
+    for job, j in zip(plan, jobs):
+        sk = evs[job.preset][0]
+        got = from_dev(j[5], sk.params.dtype)
         m, noise = sk.decrypt_with_noise(got)
-        assert (m == exp).all()
-        assert (noise < sk.params.modulus // 16).all()
+        assert (m == job.expected()).all(), job.index
+        assert (noise < sk.params.modulus // 16).all(), job.index
+        if W.digest(got) != ref[str(job.index)]["out"]:
+            bad.append(job.index)
+    assert not bad, f"jobs differing from the oracle: {bad}"
     batch.free()
     for sk, ev in evs.values():
         ev.keys.free()
