@@ -292,13 +292,17 @@ def leg_mixed(sets, steps, warmup, digests):
         ms = _timed(stream, batch.launch, steps) / steps
     ctx.synchronize()
     launches = lib().hb_ctx_launches(ctx.handle) - l0
-    ok, dig = True, (True if digests else None)
+    # digests of every job's outputs, when the committed file holds the whole plan
+    ref = digests.get("mixed", {}) if digests else {}
+    if not all(str(job.index) in ref for job in plan):
+        ref = None
+    ok, dig = True, (True if ref else None)
     for job, j in zip(plan, jobs):
         sk = sets.evs[job.preset][0]
         got = j[5].cpu().numpy().view(sk.params.dtype)
         ok = ok and bool((sk.decrypt(got) == job.expected()).all())
-        if digests:
-            dig = dig and W.digest(got) == digests["mixed"][str(job.index)]["out"]
+        if ref:
+            dig = dig and W.digest(got) == ref[str(job.index)]["out"]
     batch.free()
     per_set = {}
     for pid in (0, 1, 2):
@@ -665,8 +669,9 @@ def main():
     ok = bool((m == W.truth("nand", bits[0], bits[1])).all() and (noise < params.modulus // 16).all())
     digest_ok = None
     digests = load_json("tests", "golden", "digests_full.json")
-    if digests and rank == 0 and args.preset == W.HEADLINE_PRESET and G == W.HEADLINE_GATES:
-        ref = digests["headline"]
+    ref = digests.get("headline") if digests else None
+    if (ref and len(ref.get("out_slices", [])) * ref["slice"] == G and rank == 0
+            and args.preset == W.HEADLINE_PRESET and G == W.HEADLINE_GATES):
         digest_ok = bool(W.digest(c0) == ref["c0"] and W.digest(c1) == ref["c1"]
                          and W.slice_digests(out, ref["slice"]) == ref["out_slices"])
 

@@ -26,6 +26,7 @@ EXPORTS = [
     "hb_decrypt", "hb_ctx_create", "hb_ctx_destroy", "hb_last_error", "hb_ctx_stream",
     "hb_ctx_synchronize", "hb_ctx_hbm_in_use", "hb_keys_upload", "hb_keys_free", "hb_keys_params",
     "hb_gate", "hb_gate_device", "hb_gate_device_plain", "hb_bootstrap_lut", "hb_bootstrap_trace",
+    "hb_bootstrap_trace_device",
     "hb_ntt_forward_device", "hb_ntt_inverse_device", "hb_ntt_roundtrip_device", "hb_rgsw_upload",
     "hb_rgsw_free", "hb_external_product_device", "hb_autotune", "hb_keys_set_config",
     "hb_keys_config", "hb_keys_set_rate", "hb_batch_create", "hb_batch_launch", "hb_batch_free",
@@ -118,6 +119,7 @@ def lib():
         "hb_gate_device": (i32, [vp, vp, i32, vp, vp, vp, vp, sz]),
         "hb_gate_device_plain": (i32, [vp, vp, i32, vp, vp, vp, sz]),
         "hb_bootstrap_lut": (i32, [vp, vp, vp, vp, vp, sz]),
+        "hb_bootstrap_trace_device": (i32, [vp, vp, vp, vp, vp, sz, vp, vp]),
         "hb_bootstrap_trace": (i32, [vp, vp, vp, vp, vp, vp]),
         "hb_ntt_forward_device": (i32, [vp, i32, u32, vp, sz]),
         "hb_ntt_inverse_device": (i32, [vp, i32, u32, vp, sz]),

@@ -16,7 +16,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["hb_api.cu", "hb_serve.cu"]
+CU_SOURCES = ["hb_api.cu", "hb_serve.cu", "hb_trace.cu"]
 CPP_SOURCES = ["hb_client.cpp"]
 
 

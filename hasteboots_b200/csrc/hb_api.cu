@@ -14,6 +14,7 @@
 #include "../../include/hb_gpu.h"
 #include "hb_keygen.cuh"
 #include "hb_kernels.cuh"
+#include "hb_launch.cuh"
 #include "hb_runtime.h"
 
 using hb::BabyBear;
@@ -408,24 +409,6 @@ GateJob make_job(uint64_t P, int gate, uint32_t N, const void *c0, const void *c
   return j;
 }
 
-// The launch-independent fields of a bootstrap launch's parameters.
-template <class W>
-void boot_params(hb::BootParams<W> &prm, hb_ctx *ctx, const hb_keys *keys, const DevTables *tb) {
-  prm.bsk = (const W *)keys->bsk;
-  prm.ksk = (const W *)keys->ksk;
-  prm.tw = (const W *)tb->tw;
-  prm.itw = (const W *)tb->itw;
-  prm.n = keys->p.lwe_dim;
-  prm.len = keys->p.br_len;
-  prm.bits = keys->p.br_bits;
-  prm.ks_len = keys->p.ks_len;
-  prm.ks_bits = keys->p.ks_bits;
-  prm.ks_n = ks_dim(keys->p);
-  prm.ks_chunks = keys->p.ring_dim / prm.ks_n;
-  prm.status = ctx->d_status;
-  prm.budget = wait_budget(ctx);
-  prm.withhold = ctx->withhold_keys;
-}
 
 // Launches of at most one gate per SM (G = 1 outside the plain form) run the latency form: one gate
 // per CTA, its digits spread over the CTA's thread groups (binary LWE keys);

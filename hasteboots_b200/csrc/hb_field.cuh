@@ -14,6 +14,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #ifdef __CUDACC__
 #include "hb_gl_ptx.cuh"
@@ -148,6 +149,9 @@ struct Goldilocks {
     a.cnt = 0;
   }
   __device__ __forceinline__ static void acc_mac(Acc &a, W x, W k) { glx::mac_lazy(a.lo, a.cnt, x, k); }
+  // The carry count never overflows for the sums here (at most 2^32 products): no folds.
+  static constexpr int FOLD = 1 << 30;
+  __device__ __forceinline__ static void acc_fold(Acc &) {}
   // off = acc_offset(m) for an accumulator that took m products.
   __device__ __forceinline__ static W acc_value(const Acc &a, W off) { return glx::mac_lazy_value(a.lo, a.cnt, off); }
   // First forward stage on words below 2^15 with twiddle 2^48 (the fourth root of unity that the
@@ -194,6 +198,12 @@ struct Mont32 {
   // and one min instead of a compare, a subtract and a select.
   HB_HD static W umin(W x, W y) { return y < x ? y : x; }
   HB_HD static W canon(W x) { return umin(x, x - P); }
+  // (t + m P) / 2^32 with m = -t P^-1 mod 2^32: t 2^-32 mod P, below 2P for t < P 2^32 (no final
+  // subtraction).
+  HB_HD static uint64_t redc_lazy(uint64_t t) {
+    const uint32_t m = (uint32_t)t * PINV_NEG;
+    return (t + (uint64_t)m * P) >> 32;
+  }
   // Montgomery product a*b*2^-32 mod P for a*b < P*2^32; canonical result.
   HB_HD static W mont(W a, W b) {
     const uint64_t t = (uint64_t)a * b;
@@ -225,13 +235,41 @@ struct Mont32 {
     y = mont(sub(u, v), w);
   }
   HB_HD static W mac(W acc, W x, W k) { return add(acc, mont(x, k)); }
-  // Accumulator interface shared with Goldilocks: here every product is reduced at once.
+  // Sums of products x k (x, k < P) in the multiply-accumulate of the external product.
+  //  * WIDE (P < 2^28, DefaultFieldU32): t is a 64-bit sum of unreduced products, one 32x32 -> 64
+  //    multiply-add each (10.8 % off a DEFAULT_TERNARY launch). fold() keeps t's residue and brings
+  //    it below 2^32 (C + 1), C = 2^32 mod P, with one multiply-add, t_hi C + t_lo; FOLD products
+  //    fit between two folds (t < 2^64). The value is the Montgomery reduction of the folded t,
+  //    which is below P 2^32, so it lands in [0, 2P).
+  //  * otherwise (BabyBear, whose products reach 2^62): every product is reduced at once. A 64-bit
+  //    sum costs 32 more registers at 16 words per thread, and a 32-bit word with lazily reduced
+  //    products and carries folded back as C (6 instructions per product instead of 8) measured
+  //    1.2 % slower: the kernel is latency-bound and the fold lengthens the dependent chain.
+  static constexpr uint32_t C32 = (uint32_t)((1ull << 32) % PP);
+  static constexpr bool WIDE = PP < (1u << 28);
+  static constexpr int FOLD =
+      WIDE ? (int)((~0ull - (1ull << 32) * (C32 + 1ull)) / ((unsigned long long)PP * PP)) : (1 << 30);
   struct Acc {
-    W w;
+    typename std::conditional<WIDE, uint64_t, uint32_t>::type t;
   };
-  HB_HD static void acc_clear(Acc &a) { a.w = 0; }
-  HB_HD static void acc_mac(Acc &a, W x, W k) { a.w = mac(a.w, x, k); }
-  HB_HD static W acc_value(const Acc &a, W) { return a.w; }
+  HB_HD static void acc_clear(Acc &a) { a.t = 0; }
+  HB_HD static void acc_mac(Acc &a, W x, W k) {
+    if constexpr (WIDE) {
+      a.t += (uint64_t)x * k;
+    } else {
+      a.t = mac(a.t, x, k);
+    }
+  }
+  HB_HD static void acc_fold(Acc &a) {
+    if constexpr (WIDE) a.t = (uint64_t)(uint32_t)(a.t >> 32) * C32 + (uint32_t)a.t;
+  }
+  HB_HD static W acc_value(const Acc &a, W) {
+    if constexpr (WIDE) {
+      return canon((W)redc_lazy((uint64_t)(uint32_t)(a.t >> 32) * C32 + (uint32_t)a.t));
+    } else {
+      return a.t;
+    }
+  }
   HB_HD static W acc_offset(uint32_t) { return 0; }
   static constexpr uint64_t SMALL_FIRST_GEN = 0;  // no special first stage
   static constexpr bool RADIX8 = false;

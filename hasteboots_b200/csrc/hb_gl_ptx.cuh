@@ -75,50 +75,58 @@ __device__ __forceinline__ uint64_t mul_lazy(uint64_t a, uint64_t b) {
 // A = x2 (2^32 - 1) + (2^32 - 1 - x3) (fits 64 bits, A <= 2^64 - 2^32 < Q), lo + A = r + c 2^64 and
 // the value is r + (c - 1)(2^32 - 1) (mod Q):
 //  * c = 1: r < A <= Q - 1, so r is the canonical result;
-//  * c = 0: r - (2^32 - 1), plus Q when that borrows.
-// Adding c (2^32 - 1) first (on the multiply pipe, it cannot overflow when c = 1) makes both cases
-// one subtraction of 2^32 - 1 with a borrow fix-up.
-__device__ __forceinline__ uint64_t reduce_canon(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
-  uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
+//  * c = 0: r - (2^32 - 1) <= Q - 1 when that does not borrow, and r - 2 (2^32 - 1) + 2^64 < Q
+//    when it does (then r < 2^32 - 1).
+// m = c - 1 (0 or 2^32 - 1) makes both cases one subtraction of m with a borrow fix-up. (Adding
+// c (2^32 - 1) with two multiply-adds first and subtracting the constant measured 2.7 % slower in
+// the bootstrapping kernel: one more instruction.)
+__device__ __forceinline__ uint64_t reduce_canon_lo(uint32_t x0, uint32_t x1, uint64_t A) {
   uint32_t A0, A1;
   split(A, A0, A1);
   uint32_t r0, r1;
-  // r + c (2^32 - 1) on 32-bit halves (c (2^32 - 1) has high word 0, so the high half only takes
-  // the carry), then the subtraction of 2^32 - 1 with its borrow fix-up.
-  asm("{\n\t.reg .u32 c, bw;\n\t"
-      "add.cc.u32     %0, %2, %4;\n\t"
-      "addc.cc.u32    %1, %3, %5;\n\t"
-      "addc.u32       c, 0, 0;\n\t"
-      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %0;\n\t"
-      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t"
-      "sub.cc.u32     %0, %0, 0xFFFFFFFF;\n\t"
-      "subc.cc.u32    %1, %1, 0;\n\t"
-      "subc.u32       bw, 0, 0;\n\t"
-      "sub.cc.u32     %0, %0, bw;\n\t"
-      "subc.u32       %1, %1, 0;\n\t}"
+  asm("{\n\t.reg .u32 c, m, bw;\n\t"
+      "add.cc.u32  %0, %2, %4;\n\t"
+      "addc.cc.u32 %1, %3, %5;\n\t"
+      "addc.u32    c, 0, 0;\n\t"
+      "add.u32     m, c, 0xFFFFFFFF;\n\t"
+      "sub.cc.u32  %0, %0, m;\n\t"
+      "subc.cc.u32 %1, %1, 0;\n\t"
+      "subc.u32    bw, 0, 0;\n\t"
+      "sub.cc.u32  %0, %0, bw;\n\t"
+      "subc.u32    %1, %1, 0;\n\t}"
       : "=&r"(r0), "=&r"(r1)
       : "r"(x0), "r"(x1), "r"(A0), "r"(A1));
   return join(r0, r1);
 }
+__device__ __forceinline__ uint64_t reduce_canon(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
+  uint64_t A;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
+  return reduce_canon_lo(x0, x1, A);
+}
+// reduce_canon with x3 = 0: A = x2 (2^32 - 1) + (2^32 - 1) in one multiply-add.
+__device__ __forceinline__ uint64_t reduce_canon_x3zero(uint32_t x0, uint32_t x1, uint32_t x2) {
+  uint64_t A;
+  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, 0xFFFFFFFF;" : "=l"(A) : "r"(x2));
+  return reduce_canon_lo(x0, x1, A);
+}
 
-// reduce_canon with x0 = 0: the low limb of lo + A is A0 and cannot carry.
+// reduce_canon with x0 = 0: the low limb of lo + A is A0 and cannot carry (one instruction fewer
+// than reduce_canon; with the x3 = 0 form above, 1.0 % off the bootstrapping kernel).
 __device__ __forceinline__ uint64_t reduce_canon_x0zero(uint32_t x1, uint32_t x2, uint32_t x3) {
   uint64_t A;
   asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
   uint32_t A0, A1;
   split(A, A0, A1);
   uint32_t r0, r1;
-  asm("{\n\t.reg .u32 c, bw;\n\t"
-      "add.cc.u32     %1, %2, %3;\n\t"
-      "addc.u32       c, 0, 0;\n\t"
-      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %4;\n\t"
-      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t"
-      "sub.cc.u32     %0, %0, 0xFFFFFFFF;\n\t"
-      "subc.cc.u32    %1, %1, 0;\n\t"
-      "subc.u32       bw, 0, 0;\n\t"
-      "sub.cc.u32     %0, %0, bw;\n\t"
-      "subc.u32       %1, %1, 0;\n\t}"
+  asm("{\n\t.reg .u32 c, m, bw;\n\t"
+      "add.cc.u32  %1, %2, %3;\n\t"
+      "addc.u32    c, 0, 0;\n\t"
+      "add.u32     m, c, 0xFFFFFFFF;\n\t"
+      "sub.cc.u32  %0, %4, m;\n\t"
+      "subc.cc.u32 %1, %1, 0;\n\t"
+      "subc.u32    bw, 0, 0;\n\t"
+      "sub.cc.u32  %0, %0, bw;\n\t"
+      "subc.u32    %1, %1, 0;\n\t}"
       : "=&r"(r0), "=&r"(r1)
       : "r"(x1), "r"(A1), "r"(A0));
   return join(r0, r1);
@@ -126,7 +134,8 @@ __device__ __forceinline__ uint64_t reduce_canon_x0zero(uint32_t x1, uint32_t x2
 
 // a * b mod Q, canonical: the 128-bit product's limbs, then reduce_canon. The product is left to
 // the compiler's 64-bit multiply lowering (measured faster here than a hand-written chain of
-// 32-bit mad.lo.cc / madc.hi.cc, whose single carry flag serialises it).
+// 32-bit mad.lo.cc / madc.hi.cc, whose single carry flag serialises it, and than four
+// mad.wide.u32 with 64-bit addends and no carry flags: 1.4 % slower in the bootstrapping kernel).
 __device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
   const uint64_t lo = a * b, hi = __umul64hi(a, b);
   return reduce_canon((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
@@ -137,10 +146,10 @@ __device__ __forceinline__ uint64_t mul_canon(uint64_t a, uint64_t b) {
 // (mod Q) and nothing is reduced per product; cnt counts the carries out of 64 bits. After m calls
 // the sum of the products is acc + cnt (2^32 - 1) - m (2^32 - 1) (mod Q): mac_lazy_value.
 __device__ __forceinline__ void mac_lazy(uint64_t &acc, uint32_t &cnt, uint64_t a, uint64_t b) {
+  uint32_t x0, x1, x2, x3;
   uint32_t a0, a1, b0, b1;
   split(a, a0, a1);
   split(b, b0, b1);
-  uint32_t x0, x1, x2, x3;
   asm("mul.lo.u32     %0, %4, %6;\n\t"
       "mul.hi.u32     %1, %4, %6;\n\t"
       "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
@@ -180,7 +189,7 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t y) {
   uint32_t y0, y1;
   split(y, y0, y1);
   if constexpr (E < 32) {
-    return reduce_canon(y0 << E, __funnelshift_l(y0, y1, E), y1 >> (32 - E), 0u);
+    return reduce_canon_x3zero(y0 << E, __funnelshift_l(y0, y1, E), y1 >> (32 - E));
   } else if constexpr (E == 32) {
     return reduce_canon_x0zero(y0, y1, 0u);
   } else if constexpr (E < 64) {

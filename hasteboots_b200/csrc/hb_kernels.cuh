@@ -295,6 +295,17 @@ __device__ __forceinline__ void digits_reg(W (&x)[V], const W (&e)[V], uint32_t 
   }
 }
 
+// A lazy accumulator that already took `nprod` products must be folded (F::acc_fold) before the
+// next one: every F::FOLD products (never for fields whose accumulators need no folds).
+template <class F>
+__device__ __forceinline__ bool fold_due(uint32_t nprod) {
+  if constexpr (F::FOLD >= (1 << 20)) {
+    return false;
+  } else {
+    return nprod != 0 && nprod % F::FOLD == 0;
+  }
+}
+
 template <class F, int LOGN, int T, int G, int S>
 __global__ void __launch_bounds__(G * T, 1)
     ext_product_kernel(const typename F::W *__restrict__ rlwe_in, typename F::W *__restrict__ rlwe_out,
@@ -351,6 +362,7 @@ __global__ void __launch_bounds__(G * T, 1)
       F::acc_clear(acc_a[v]);
       F::acc_clear(acc_b[v]);
     }
+    uint32_t nprod = 0;  // products in the accumulators since the last fold
     for (int part = 0; part < 2; ++part) {
       W e[V];
       if (active) {
@@ -366,12 +378,20 @@ __global__ void __launch_bounds__(G * T, 1)
         }
         const W *k = pipe.acquire();
         if (active) {
+          if (fold_due<F>(nprod)) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              F::acc_fold(acc_a[v]);
+              F::acc_fold(acc_b[v]);
+            }
+          }
 #pragma unroll
           for (int v = 0; v < V; ++v) {
             F::acc_mac(acc_a[v], x[v], k[v * T + t]);
             F::acc_mac(acc_b[v], x[v], k[N + v * T + t]);
           }
         }
+        ++nprod;
         if (!pipe.release(src, t, sync)) goto aborted;
       }
     }
@@ -415,8 +435,11 @@ struct BootParams {
   int *status;
   long long budget;
   int withhold;  // test hook: issue no key-chunk copy, so the first wait runs out (bounded)
-  W *trace;      // bootstrap_dp_kernel with one gate: the accumulator after every blind-rotation
-                 // step, [n][a | b][N] canonical words; null records nothing
+  W *trace;      // the accumulator after every blind-rotation step, [gate][n][a | b][N] canonical
+                 // words (bootstrap_dp_kernel: one gate; bootstrap_kernel: its TRACE variant, one
+                 // job); null records nothing
+  uint8_t *digits;  // bootstrap_kernel's TRACE variant: every step's gadget digits of E.a then E.b,
+                    // [gate][n][2][len][N] bytes (bases up to 2^8); null records nothing
 };
 
 // Shared memory needed by bootstrap_kernel: twiddles (2N words), S key-chunk stages (2N words
@@ -450,7 +473,10 @@ __host__ __device__ constexpr int boot_stages() {
 // untransformed NTT-domain monomial (:93-100), which this kernel does not reproduce.
 // KSC: key switch in ks_chunks chunks of n' = next_pow2(n) < N words; without it the key switch is
 // the single chunk n' = N of the reference presets, with no chunk bookkeeping in the kernel.
-template <class F, int LOGN, int T, int G, int S, bool TERN = false, bool KSC = false>
+// TRACE (binary LWE key, one job): every gate also writes the accumulator after each blind-rotation
+// step to p.trace and, when p.digits is set, each step's gadget digits to p.digits (the witness of
+// vfhe's traced bootstrap, vfhe/src/bfhe/evaluate.rs:47-141).
+template <class F, int LOGN, int T, int G, int S, bool TERN = false, bool KSC = false, bool TRACE = false>
 __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T, kBootPingPong>;
@@ -582,6 +608,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
         F::acc_clear(acc_y1[v]);
       }
     }
+    uint32_t nprod = 0;  // products in the accumulators since their last fold or clear
     const uint32_t phases = 2 * n + ks_chunks;
     for (uint32_t ph = 0; ph < phases; ++ph) {
       const bool ks = KSC ? ph >= 2 * n : ph == 2 * n;
@@ -641,16 +668,36 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
         if (active) {
           const uint32_t sh = j * bits;
           digits<W, V, T>(x, ebuf, t, sh, (uint32_t)mask);
+          if constexpr (TRACE) {
+            // digit j of E.part at step ph / 2: coefficient v T + t is in x[v]
+            if (!ks && p.digits) {
+              uint8_t *dd = p.digits + ((((size_t)gate * n + (ph >> 1)) * 2 + part) * p.len + j) * N;
+#pragma unroll
+              for (int v = 0; v < V; ++v) dd[v * T + t] = (uint8_t)x[v];
+            }
+          }
           NT::forward_small(x, xbuf, ping, s_tw, t, sync);
         }
         const W *k = pipe.acquire();
         if (active) {
+          if (fold_due<F>(nprod)) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              F::acc_fold(acc_x[v]);
+              F::acc_fold(acc_y[v]);
+              if constexpr (TERN) {
+                F::acc_fold(acc_x1[v]);
+                F::acc_fold(acc_y1[v]);
+              }
+            }
+          }
 #pragma unroll
           for (int v = 0; v < V; ++v) {
             F::acc_mac(acc_x[v], x[v], k[v * T + t]);
             F::acc_mac(acc_y[v], x[v], k[N + v * T + t]);
           }
         }
+        ++nprod;
         if (!pipe.release(src, t, sync)) goto aborted;
         if constexpr (TERN) {
           if (!ks) {  // the same digit against RGSW(s_i == -1)
@@ -712,6 +759,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             }
             sync();  // ebuf written (h even) or read (h odd) by the whole group
           }
+          nprod = 0;
           continue;
         }
       }
@@ -734,6 +782,8 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             for (int v = 0; v < V; ++v) {
               const int k = NT::natural_pos(t, v);
               y[k] = F::add(y[k], F::canon(f[v]));  // RLWE::add_assign_element_wise
+              if constexpr (TRACE)
+                p.trace[(((size_t)gate * n + (ph >> 1)) * 2 + h) * N + k] = F::canon(y[k]);
             }
           } else {
             // extract_partial_lwe_locally (lattice/src/rlwe.rs:393-402): a' = [A0, -A_{N-1}, ...],
@@ -764,6 +814,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
           }
         }
       }
+      nprod = 0;
       sync();
     }
   }
@@ -964,6 +1015,7 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         F::acc_clear(ax[v]);
         F::acc_clear(ay[v]);
       }
+      uint32_t nprod = 0;  // products in ax / ay since their last fold
       for (uint32_t d = gg; d < nd; d += C * D) {
         const uint32_t part = ks ? 0 : d / L, j = ks ? d % p.ks_len : d % L;
         W x[V];
@@ -1002,11 +1054,19 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
           }
         }
         NT::forward_small(x, xbuf, ping, s_tw, t, sync);
+        if (fold_due<F>(nprod)) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            F::acc_fold(ax[v]);
+            F::acc_fold(ay[v]);
+          }
+        }
 #pragma unroll
         for (int v = 0; v < V; ++v) {
           F::acc_mac(ax[v], x[v], k[v * T + t]);
           F::acc_mac(ay[v], x[v], k[N + v * T + t]);
         }
+        ++nprod;
       }
       sync();  // the group's last exchange has been read: its buffers take the partial sums
       {

@@ -71,6 +71,8 @@ int scratch(hb_ctx *ctx, Scratch &s, size_t bytes);
 int tables(hb_ctx *ctx, int field_id, uint32_t logn, DevTables **out, uint32_t logv = 4);
 int check_status(hb_ctx *ctx);
 long long wait_budget(const hb_ctx *ctx);
+// The key switch's dimension n' = next_pow2(n) (fhe_core/src/key_switch/rlwe.rs:40-43).
+uint32_t ks_dim(const hb_params &p);
 // One persistent bootstrapping launch over a device job table (full grid, the keys' variant).
 int launch_set(hb_ctx *ctx, hb_keys *keys, int gates_per_cta, const hb::GateJob *djobs, int njobs,
                uint32_t batches, cudaStream_t stream);

@@ -339,6 +339,33 @@ class Evaluator:
         return out, trace
 
 
+    def bootstrap_with_trace_batch(self, c, lut, digits=True):
+        """bootstrap of a batch of ciphertexts (one persistent launch) with, per ciphertext, the
+        accumulator after every blind-rotation step and, with digits=True, every step's gadget
+        digits of (X^a_i - 1) ACC (hb_bootstrap_trace_device). Host arrays in; returns
+        (out [count, n + 1], acc [count, n, 2N], digits [count, n, 2, l, N] uint8 or None)."""
+        import torch
+        dt = self.params.dtype
+        raw = self.params.raw
+        n, N, L = raw.lwe_dim, raw.ring_dim, raw.br_len
+        c = np.ascontiguousarray(c, dt).reshape(-1, n + 1)
+        count = len(c)
+        tdt = torch.int64 if dt == np.uint64 else torch.int32
+        ivt = np.int64 if dt == np.uint64 else np.int32
+        dc = torch.from_numpy(c.view(ivt).copy()).cuda()
+        dl = torch.from_numpy(np.ascontiguousarray(lut, dt).view(ivt).copy()).cuda()
+        dout = torch.zeros_like(dc)
+        dacc = torch.zeros((count, n, 2 * N), dtype=tdt, device="cuda")
+        ddig = torch.zeros((count, n, 2, L, N), dtype=torch.uint8, device="cuda") if digits else None
+        torch.cuda.synchronize()
+        check(lib().hb_bootstrap_trace_device(self.ctx.handle, self.keys.handle, _ptr(dc), _ptr(dl),
+                                              _ptr(dout), count, _ptr(dacc), _ptr(ddig)),
+              "bootstrap_with_trace_batch", self.ctx.handle)
+        self.ctx.synchronize()
+        return (dout.cpu().numpy().view(dt), dacc.cpu().numpy().view(dt),
+                ddig.cpu().numpy() if digits else None)
+
+
 # ------------------------------------------------------------------------------------------------
 # Autotuning and mixed-set batches
 # ------------------------------------------------------------------------------------------------

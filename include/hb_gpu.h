@@ -178,6 +178,22 @@ int hb_bootstrap_lut(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut,
  * (HB_ERR_UNSUPPORTED for a ternary one). */
 int hb_bootstrap_trace(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut, void *out,
                        void *acc_trace);
+/* The traced bootstrap of vfhe (vfhe/src/bfhe/evaluate.rs:47-141) for a batch of count ciphertexts
+ * sharing one LUT polynomial, in one persistent launch (two gates per CTA). Per gate g:
+ *  - acc_trace[g][i] = the accumulator after blind-rotation step i, n x 2N canonical words (a then
+ *    b): AccTrace's rows (trace/src/acc_trace.rs, blind_rotate_w_trace,
+ *    fhe_core/src/blind_rotation/rlwe/binary.rs:106-205);
+ *  - digit_trace[g][i][part][j] (may be NULL) = the N unsigned gadget digits j of E.a (part 0) and
+ *    E.b (part 1), E = (X^a_i - 1) ACC, one byte each, [count][n][2][l][N]: the bit polynomials
+ *    of SumHadamardTrace (append_bit_poly in mul_polynomial_inplace_fast_w_traces,
+ *    lattice/src/gadget/rlwe.rs:426-457); a step with a_i = 0 has E = 0 and zero digits.
+ * The digits' NTTs and the NTT-domain key rows the reference records as well are not produced:
+ * their slot order is concrete-ntt's. Device pointers; c and out are [count][n + 1] words, lut N
+ * words; enqueued on the context stream (hb_ctx_synchronize reports device-side waits that ran
+ * out). Binary LWE keys; digit traces need a gadget base of at most 2^8 (every preset's).
+ * HB_ERR_UNSUPPORTED otherwise. */
+int hb_bootstrap_trace_device(hb_ctx *ctx, hb_keys *keys, const void *c, const void *lut, void *out,
+                              size_t count, void *acc_trace, void *digit_trace);
 
 /* ---- NTT table trait and external product (device slices) ---------------------------------- */
 

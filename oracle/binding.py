@@ -111,7 +111,7 @@ def lib():
         L.orc_bootstrap_lut.argtypes = [P, vp, vp, vp, vp, vp, sz, i32]
         L.orc_modswitch.argtypes = [P, vp, vp]
         L.orc_blind_rotate.argtypes = [P, vp, vp, vp, ctypes.c_uint32, vp]
-        L.orc_blind_rotate_trace.argtypes = [P, vp, vp, vp, vp]
+        L.orc_blind_rotate_trace.argtypes = [P, vp, vp, vp, vp, vp]
         L.orc_ntt_roundtrip.argtypes = [i32, ctypes.c_uint32, vp, vp]
         L.orc_negacyclic_mul.argtypes = [i32, ctypes.c_uint32, vp, vp, vp, i32]
         L.orc_external_product.argtypes = [i32, ctypes.c_uint32, ctypes.c_uint32,
@@ -250,16 +250,18 @@ def blind_rotate(keys, c, lut, steps):
     return out
 
 
-def blind_rotate_trace(keys, c, lut):
-    """The accumulator after every blind-rotation step: [n, 2N] (a then b, canonical)."""
+def blind_rotate_trace(keys, c, lut, digits=False):
+    """The accumulator after every blind-rotation step: [n, 2N] (a then b, canonical); with
+    digits=True also every step's gadget digits of E.a then E.b, [n, 2, l, N] uint8."""
     p = keys.p
     dt = dtype_of(p.field_id)
     c = np.ascontiguousarray(c, dtype=dt)
     lut = np.ascontiguousarray(lut, dtype=dt)
     out = np.zeros((p.lwe_dim, 2 * p.ring_dim), dt)
+    dig = np.zeros((p.lwe_dim, 2, p.br_len, p.ring_dim), np.uint8) if digits else None
     _check(lib().orc_blind_rotate_trace(ctypes.byref(p), _ptr(keys.bsk), _ptr(c), _ptr(lut),
-                                        _ptr(out)), "blind_rotate_trace")
-    return out
+                                        _ptr(out), _ptr(dig)), "blind_rotate_trace")
+    return (out, dig) if digits else out
 
 
 def ntt_roundtrip(field_id, log_n, x):

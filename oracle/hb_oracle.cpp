@@ -726,10 +726,12 @@ void monomial_sub_one(const typename F::T *y, typename F::T *x, uint32_t N, uint
 }
 
 // RLWE::mul_assign_ntt_rgsw (lattice/src/rlwe.rs:573-596): c_neg_s_m x E.a + c_m x E.b, then INTT.
-// rgsw_ntt layout [part][j][ab][N].
+// rgsw_ntt layout [part][j][ab][N]. With `digits` (bits <= 8), the coefficient-domain gadget digits
+// go to digits[(part L + j) N + k]: the bit polynomials that the traced product records
+// (mul_polynomial_inplace_fast_w_traces, lattice/src/gadget/rlwe.rs:426-457, append_bit_poly).
 template <class F>
 void external_product(const Ntt<F> &ntt, uint32_t bits, uint32_t L, const typename F::T *rgsw_ntt,
-                      typename F::T *ea, typename F::T *eb) {
+                      typename F::T *ea, typename F::T *eb, uint8_t *digits = nullptr) {
   using T = typename F::T;
   using Acc = typename F::Acc;
   const uint32_t N = ntt.n;
@@ -746,6 +748,8 @@ void external_product(const Ntt<F> &ntt, uint32_t bits, uint32_t L, const typena
     std::copy(src, src + N, poly);
     for (uint32_t j = 0; j < L; ++j) {
       decompose_step<F>(poly, digit, N, bits);
+      if (digits)
+        for (uint32_t k = 0; k < N; ++k) digits[((size_t)part * L + j) * N + k] = (uint8_t)digit[k];
       ntt.forward(digit);
       const T *ka = rgsw_ntt + ((size_t)part * L + j) * 2 * N;
       const T *kb = ka + N;
@@ -779,11 +783,12 @@ void trace_row(const typename F::T *acc_a, const typename F::T *acc_b, uint32_t 
 // BinaryBlindRotationKey::blind_rotate (fhe_core/src/blind_rotation/rlwe/binary.rs:28-104).
 // acc_a/acc_b hold the reference's representation of the accumulator. With `trace`, the accumulator
 // after every step i goes to trace[i] (blind_rotate_w_trace, binary.rs:106-205, which does not skip
-// a_i = 0; such a step leaves the accumulator unchanged).
+// a_i = 0; such a step leaves the accumulator unchanged). With `digits`, step i's gadget digits of
+// E.a and E.b go to digits[i][2 L][N] (zero for a step with a_i = 0, whose E is zero).
 template <class F>
 void blind_rotate(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T *lut_in,
                   uint32_t steps, typename F::T *acc_a, typename F::T *acc_b,
-                  typename F::T *trace = nullptr) {
+                  typename F::T *trace = nullptr, uint8_t *digits = nullptr) {
   using T = typename F::T;
   const Dims &d = ek.d;
   const uint32_t N = d.N;
@@ -813,7 +818,8 @@ void blind_rotate(const EvalKey<F> &ek, const uint32_t *ms, const typename F::T 
     if (ai != 0) {  // binary.rs:70
       monomial_sub_one<F>(acc_a, ea.data(), N, ai);
       monomial_sub_one<F>(acc_b, eb.data(), N, ai);
-      external_product<F>(ntt, d.bits, d.len, ek.bsk_ntt.data() + i * entry, ea.data(), eb.data());
+      external_product<F>(ntt, d.bits, d.len, ek.bsk_ntt.data() + i * entry, ea.data(), eb.data(),
+                          digits ? digits + (size_t)i * 2 * d.len * N : nullptr);
       // RLWE::add_assign_element_wise (lattice/src/rlwe.rs:287-290)
       for (uint32_t k = 0; k < N; ++k) {
         acc_a[k] = F::add_ref(acc_a[k], ea[k]);
@@ -1242,7 +1248,7 @@ int orc_modswitch(const orc_params *p, const void *c, uint32_t *out) {
 
 // The accumulator after `steps` steps (acc_out: 2N words), and with `trace` every step's row.
 static int blind_rotate_probe(const orc_params *p, const void *bsk, const void *c, const void *lut,
-                       uint32_t steps, void *acc_out, void *trace) {
+                       uint32_t steps, void *acc_out, void *trace, uint8_t *digits = nullptr) {
   Dims d;
   if (!dims_of(p, d)) return -1;
   ORC_DISPATCH(p, {
@@ -1263,7 +1269,7 @@ static int blind_rotate_probe(const orc_params *p, const void *bsk, const void *
     if (d.pairs == 2)
       blind_rotate_ternary<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N, (T *)trace);
     else
-      blind_rotate<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N, (T *)trace);
+      blind_rotate<F>(*ek, ms.data(), (const T *)lut, used, acc, acc + d.N, (T *)trace, digits);
     for (uint32_t k = 0; k < 2 * d.N; ++k) acc[k] = F::canon(acc[k]);
   });
   return 0;
@@ -1275,10 +1281,13 @@ int orc_blind_rotate(const orc_params *p, const void *bsk, const void *c, const 
 }
 
 int orc_blind_rotate_trace(const orc_params *p, const void *bsk, const void *c, const void *lut,
-                           void *trace_out) {
+                           void *trace_out, void *digits_out) {
   if (!p || !trace_out) return -1;
+  if (digits_out && (p->br_bits > 8 || p->lwe_ternary)) return -1;
+  if (digits_out)
+    std::memset(digits_out, 0, (size_t)p->lwe_dim * 2 * p->br_len * p->ring_dim);
   std::vector<uint64_t> acc(2 * (size_t)p->ring_dim);  // room for either word size
-  return blind_rotate_probe(p, bsk, c, lut, p->lwe_dim, acc.data(), trace_out);
+  return blind_rotate_probe(p, bsk, c, lut, p->lwe_dim, acc.data(), trace_out, (uint8_t *)digits_out);
 }
 
 int orc_ntt_roundtrip(int field_id, uint32_t log_n, const void *in, void *out) {

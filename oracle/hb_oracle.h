@@ -110,9 +110,11 @@ int orc_modswitch(const orc_params *p, const void *c, uint32_t *out);
 int orc_blind_rotate(const orc_params *p, const void *bsk, const void *c, const void *lut,
                      uint32_t steps, void *acc_out);
 /* The accumulator after every one of the n steps in one pass: n rows of 2N words (a then b,
- * canonical), the rows of the AccTrace that vfhe's traced bootstrap records. */
+ * canonical), the rows of the AccTrace that vfhe's traced bootstrap records. digits_out (may be
+ * NULL; binary LWE keys with B <= 2^8): every step's unsigned gadget digits of E.a then E.b,
+ * [n][2][l][N] bytes, the bit polynomials of its SumHadamardTrace (zero for a step with a_i = 0). */
 int orc_blind_rotate_trace(const orc_params *p, const void *bsk, const void *c, const void *lut,
-                           void *trace_out);
+                           void *trace_out, void *digits_out);
 
 /* Negacyclic NTT round trip / product checks (N = 1<<log_n). */
 int orc_ntt_roundtrip(int field_id, uint32_t log_n, const void *in, void *out);

@@ -177,3 +177,44 @@ def test_blind_rotation_trace_rows(oracle, oracle_keys):
         for i in range(1, n):
             if ms[i] == 0:
                 assert (rows[i] == rows[i - 1]).all(), (pid, i)
+
+
+def _rot_sub(y, r, q):
+    """(X^r - 1) y in Z_q[X]/(X^N + 1), canonical (numpy object arithmetic)."""
+    N = len(y)
+    y = [int(v) for v in y]
+    x = [0] * N
+    for k in range(N):
+        s = k - r
+        x[k] = y[s] if s >= 0 else (q - y[s + N]) % q if s >= -N else y[s + 2 * N]
+    return [(x[k] - y[k]) % q for k in range(N)]
+
+
+def test_blind_rotation_trace_digits(oracle, oracle_keys):
+    """The trace's gadget digits of every step are below B, recombine (sum d_j B^j) to
+    E = (X^a_i - 1) ACC computed without any NTT from the previous accumulator row, and are zero on
+    steps whose rotation a_i is zero (binary LWE keys; the unsigned LSB-first decomposition of
+    native_polynomial.rs:340-348)."""
+    g = np.load(GOLDEN)
+    for pid in (0, 1):
+        name = oracle.SET_NAMES[pid]
+        k = oracle_keys(pid)
+        q, N, L, b = oracle.MODULUS[k.p.field_id], k.p.ring_dim, k.p.br_len, k.p.br_bits
+        c0, c1 = g[f"{name}/c0"][0], g[f"{name}/c1"][0]
+        s = np.array([(int(a) + int(x)) % q for a, x in zip(c0, c1)], c0.dtype)
+        lut = oracle.lut_poly(k.p.field_id, "nand", N)
+        rows, dig = oracle.blind_rotate_trace(k, s, lut, digits=True)
+        assert dig.shape == (k.p.lwe_dim, 2, L, N) and int(dig.max()) < (1 << b)
+        ms = oracle.modswitch(k.p, s)
+        weights = [1 << (b * j) for j in range(L)]
+        for i in (1, 2, 57, k.p.lwe_dim - 1):
+            if ms[i] == 0:
+                assert not dig[i].any()
+                continue
+            prev = rows[i - 1]
+            for part in (0, 1):
+                e = _rot_sub(prev[part * N:(part + 1) * N], int(ms[i]), q)
+                got = [sum(int(dig[i, part, j, c]) * weights[j] for j in range(L)) for c in range(N)]
+                assert got == e, (pid, i, part)
+        zero = [i for i in range(k.p.lwe_dim) if ms[i] == 0]
+        assert all(not dig[i].any() for i in zero)
