@@ -1,0 +1,79 @@
+"""The 32-bit fields' multiply-accumulate (hasteboots_b200/csrc/hb_field.cuh, Mont32::Acc) compiled
+for the host with g++ and checked against exact integer arithmetic: DefaultFieldU32's 64-bit
+unreduced sums with residue-keeping folds (forced here at every spacing up to FOLD, and at the
+extreme word values), and BabyBear's per-product reduction. The value of a sum of products x k is
+sum(x k) 2^-32 mod P, since the keys it multiplies are stored in Montgomery form."""
+
+import os
+import random
+import subprocess
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "hasteboots_b200", "csrc")
+
+DRIVER = r"""
+#include <cstdio>
+#include <cstdlib>
+#include "hb_field.cuh"
+template <class F>
+void run() {
+  using W = typename F::W;
+  unsigned n, fold;
+  while (scanf("%u %u", &n, &fold) == 2) {
+    typename F::Acc a;
+    F::acc_clear(a);
+    for (unsigned i = 0; i < n; ++i) {
+      unsigned x, k;
+      if (scanf("%u %u", &x, &k) != 2) return;
+      if (fold && i && i % fold == 0) F::acc_fold(a);
+      F::acc_mac(a, (W)x, (W)k);
+    }
+    printf("%u\n", (unsigned)F::acc_value(a, 0));
+  }
+}
+int main(int argc, char **argv) {
+  if (argv[1][0] == 'd') run<hb::DefaultFieldU32>(); else run<hb::BabyBear>();
+  printf("FOLD %d\n", argv[1][0] == 'd' ? hb::DefaultFieldU32::FOLD : hb::BabyBear::FOLD);
+  return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def driver():
+    d = tempfile.mkdtemp()
+    src, exe = os.path.join(d, "acc.cpp"), os.path.join(d, "acc")
+    open(src, "w").write(DRIVER)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", CSRC, src, "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("field,P", [("d", 132120577), ("b", 0x78000001)])
+def test_accumulate_matches_exact_sums(driver, field, P):
+    rng = random.Random(7)
+    cases = []
+    for n in (1, 2, 3, 8, 18, 27, 64):
+        for fold in (0, 1, 2, 5, 16, 30):
+            rows = [(rng.randrange(P), rng.randrange(P)) for _ in range(n)]
+            cases.append((n, fold, rows))
+    # the largest words, where the bounds are tight
+    cases.append((40, 30, [(P - 1, P - 1)] * 40))
+    cases.append((27, 0, [(P - 1, P - 1)] * 27))
+    text = "".join(f"{n} {fold} " + " ".join(f"{x} {k}" for x, k in rows) + "\n" for n, fold, rows in cases)
+    out = subprocess.run([driver, field], input=text, capture_output=True, text=True, check=True).stdout.split()
+    fold_max = int(out[-1])
+    assert out[-2] == "FOLD"
+    rinv = pow(1 << 32, -1, P)
+    for (n, fold, rows), got in zip(cases, out[:-2]):
+        if field == "d":
+            # a case only makes sense where the products between folds stay within FOLD
+            span = fold if fold else n
+            if span > fold_max:
+                continue
+        expect = sum(x * k for x, k in rows) * rinv % P
+        assert int(got) == expect, (n, fold)
+    if field == "d":
+        assert fold_max >= 27  # DEFAULT_TERNARY's key switch sums 27 products without a fold
