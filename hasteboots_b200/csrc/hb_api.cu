@@ -416,11 +416,11 @@ GateJob make_job(uint64_t P, int gate, uint32_t N, const void *c0, const void *c
 // per gate while the whole launch fits the GPU's co-resident clusters.
 constexpr int kDpCluster = 4;
 
-template <class F, int LOGN, int T, int C, bool KSC>
+template <class F, int LOGN, int T, int C, bool KSC, bool TERN = false>
 int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream, int *max_clusters) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T>();
-  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D, C, KSC>;
+  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D, C, KSC, TERN>;
   const size_t smem = hb::dp_smem_bytes<W, N, D, C>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
@@ -456,7 +456,7 @@ int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStrea
   return HB_OK;
 }
 
-template <class F, int LOGN, int T, bool KSC>
+template <class F, int LOGN, int T, bool KSC, bool TERN = false>
 int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t stream) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
@@ -465,7 +465,7 @@ int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t strea
   const DevTables &tbw = ctx->tables[F::FIELD_ID][LOGN][LOGVW];
   if (!tbw.itw) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
   prm.itw_w = (const W *)tbw.itw;
-  if constexpr (sizeof(W) == 8) {
+  if constexpr (sizeof(W) == 8 && !TERN) {
     std::atomic<int> &cached = ctx->dp_clusters[T == 128 ? 1 : 0];
     int m = cached.load();
     if (m < 0) {  // the same shared memory and threads with or without KSC
@@ -475,7 +475,7 @@ int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t strea
     }
     if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, kDpCluster, KSC>(ctx, prm, stream, nullptr);
   }
-  return launch_dp_c<F, LOGN, T, 1, KSC>(ctx, prm, stream, nullptr);
+  return launch_dp_c<F, LOGN, T, 1, KSC, TERN>(ctx, prm, stream, nullptr);
 }
 
 template <class F, int LOGN, int T, int G, bool TERN, bool KSC>
@@ -513,7 +513,7 @@ int launch_boot(hb_ctx *ctx, hb_keys *keys, std::vector<GateJob> &jobs, bool pla
     prm.jobs = djobs;
     prm.njobs = (int)jobs.size();
     prm.total_batches = batches;
-    if constexpr (G == 1 && !TERN) return launch_dp<F, LOGN, T, KSC>(ctx, prm, ctx->stream);
+    if constexpr (G == 1) return launch_dp<F, LOGN, T, KSC, TERN>(ctx, prm, ctx->stream);
     kern<<<grid, block, smem, ctx->stream>>>(prm);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap launch");
@@ -610,7 +610,7 @@ int launch_table(hb_ctx *ctx, hb_keys *keys, const GateJob *djobs, int njobs, ui
   prm.jobs = djobs;
   prm.njobs = njobs;
   prm.total_batches = batches;
-  if constexpr (G == 1 && !TERN) return launch_dp<F, LOGN, T, KSC>(ctx, prm, stream);
+  if constexpr (G == 1) return launch_dp<F, LOGN, T, KSC, TERN>(ctx, prm, stream);
   constexpr int S = hb::boot_stages<W, N, G>();
   auto kern = hb::bootstrap_kernel<F, LOGN, T, G, S, TERN, KSC>;
   const size_t smem = hb::boot_smem_bytes<W, N, G, S>(prm.n);

@@ -295,16 +295,45 @@ __device__ __forceinline__ void digits_reg(W (&x)[V], const W (&e)[V], uint32_t 
   }
 }
 
-// A lazy accumulator that already took `nprod` products must be folded (F::acc_fold) before the
-// next one: every F::FOLD products (never for fields whose accumulators need no folds).
-template <class F>
-__device__ __forceinline__ bool fold_due(uint32_t nprod) {
-  if constexpr (F::FOLD >= (1 << 20)) {
+// A lazy accumulator that already took `nprod` products must be folded (acc_fold) before the
+// next one: every FOLD products (never for accumulators that need no folds).
+template <int FOLD>
+__device__ __forceinline__ bool fold_due_n(uint32_t nprod) {
+  if constexpr (FOLD >= (1 << 20)) {
     return false;
   } else {
-    return nprod != 0 && nprod % F::FOLD == 0;
+    return nprod != 0 && nprod % FOLD == 0;
   }
 }
+template <class F>
+__device__ __forceinline__ bool fold_due(uint32_t nprod) {
+  return fold_due_n<F::FOLD>(nprod);
+}
+
+// Accumulator of the latency form, whose groups each sum only a few products per phase: the
+// field's lazy accumulator for Goldilocks, and for the 32-bit fields a word reduced at every
+// product (their 64-bit sums cost 32 registers at 16 words per thread, more than their
+// instructions save on a few products).
+template <class F, bool REDUCED = sizeof(typename F::W) == 4>
+struct FewAcc {
+  using A = typename F::Acc;
+  static constexpr int FOLD = F::FOLD;
+  __device__ __forceinline__ static void clear(A &a) { F::acc_clear(a); }
+  __device__ __forceinline__ static void mac(A &a, typename F::W x, typename F::W k) { F::acc_mac(a, x, k); }
+  __device__ __forceinline__ static void fold(A &a) { F::acc_fold(a); }
+  __device__ __forceinline__ static typename F::W value(const A &a, typename F::W off) { return F::acc_value(a, off); }
+};
+template <class F>
+struct FewAcc<F, true> {
+  struct A {
+    typename F::W w;
+  };
+  static constexpr int FOLD = 1 << 30;
+  __device__ __forceinline__ static void clear(A &a) { a.w = 0; }
+  __device__ __forceinline__ static void mac(A &a, typename F::W x, typename F::W k) { a.w = F::mac(a.w, x, k); }
+  __device__ __forceinline__ static void fold(A &) {}
+  __device__ __forceinline__ static typename F::W value(const A &a, typename F::W) { return a.w; }
+};
 
 template <class F, int LOGN, int T, int G, int S>
 __global__ void __launch_bounds__(G * T, 1)
@@ -890,12 +919,20 @@ __device__ __forceinline__ const W *cluster_peer(const W *p, uint32_t rank) {
 // KSC: the key switch in ks_chunks chunks of n' < N words (as bootstrap_kernel's KSC): digit d of
 // the key-switch phase is digit d mod l_ks of chunk d / l_ks, whose source words are formed from
 // the accumulator where the digit is taken, and the extraction reads every (N/n')-th coefficient.
-template <class F, int LOGN, int T, int D, int C = 1, bool KSC = false>
+//
+// TERN (ternary LWE key, one CTA per gate): in a blind-rotation step the first half of the groups
+// multiplies all 2l digits by RGSW(s_i == 1), the second half by RGSW(s_i == -1), so no group
+// holds two sets of sums. Each CTA half then reads both pairs' sums of its polynomial,
+// inverse-transforms the pair-1 sum into a stage and the pair-0 sum in registers, and adds
+// INTT(pair-0 sum) - X^(2N - a_i) INTT(pair-1 sum) to the accumulator: the evaluation key
+// RGSW_0 + RGSW_1 (-X^-a_i) of bootstrap_kernel's TERN step (ternary.rs:78-114).
+template <class F, int LOGN, int T, int D, int C = 1, bool KSC = false, bool TERN = false>
 __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T>;
   constexpr int N = 1 << LOGN, V = NT::V, NT_ALL = D * T;
   static_assert(D >= 2 && D % 2 == 0, "two half-CTA groups transform the a and b sums");
+  static_assert(!TERN || (C == 1 && D >= 4), "ternary keys: one CTA per gate, a pair per CTA half");
   constexpr int TW = D / 2 * T;  // threads of a half-CTA group
   using NW = GroupNtt<F, LOGN, TW>;
   constexpr int VW = NW::V;
@@ -932,7 +969,11 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
   const uint32_t n = p.n, L = p.len, two_n = 2 * N;
   // products each group accumulates per phase (digits gg, gg + C D, ...), for the lazy offsets
   const uint32_t nd_br = 2 * L, nd_ks = (KSC ? p.ks_chunks : 1) * p.ks_len;
-  const uint32_t my_br = (uint32_t)gg < nd_br ? (nd_br - 1 - gg) / (C * D) + 1 : 0;
+  // TERN: a blind-rotation step's digits go to the D/2 groups of the CTA half of the group's pair
+  const uint32_t br_lanes = TERN ? D / 2 : C * D;
+  const uint32_t br_first = TERN ? (uint32_t)(g % (D / 2)) : (uint32_t)gg;
+  const uint32_t br_pair = TERN ? (uint32_t)(g / (D / 2)) : 0;
+  const uint32_t my_br = br_first < nd_br ? (nd_br - 1 - br_first) / br_lanes + 1 : 0;
   const uint32_t my_ks = (uint32_t)gg < nd_ks ? (nd_ks - 1 - gg) / (C * D) + 1 : 0;
   const W off_br = F::acc_offset(my_br);
   const W off_ks = F::acc_offset(my_ks);
@@ -1009,14 +1050,15 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
       const uint32_t nd = ks ? nd_ks : nd_br;
       const uint32_t bits = ks ? p.ks_bits : p.bits;
       const uint32_t mask = (1u << bits) - 1;
-      typename F::Acc ax[V], ay[V];
+      using FA = FewAcc<F>;
+      typename FA::A ax[V], ay[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        F::acc_clear(ax[v]);
-        F::acc_clear(ay[v]);
+        FA::clear(ax[v]);
+        FA::clear(ay[v]);
       }
       uint32_t nprod = 0;  // products in ax / ay since their last fold
-      for (uint32_t d = gg; d < nd; d += C * D) {
+      for (uint32_t d = ks ? (uint32_t)gg : br_first; d < nd; d += ks ? C * D : br_lanes) {
         const uint32_t part = ks ? 0 : d / L, j = ks ? d % p.ks_len : d % L;
         W x[V];
         if (KSC && ks) {
@@ -1041,7 +1083,9 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         } else {
           digits<W, V, T>(x, s_e + part * N, t, j * bits, mask);
         }
-        const W *k = ks ? p.ksk + (size_t)d * 2 * N : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
+        const W *k = ks     ? p.ksk + (size_t)d * 2 * N
+                     : TERN ? p.bsk + ((((size_t)ph * 2 + br_pair) * 2 + part) * L + j) * 2 * N
+                            : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
         // Goldilocks keys (191-310 MB) exceed L2: start the key row's way from HBM into L2 while the
         // digit transform runs (the loads below come after the transform's barriers, so they cannot
         // be issued earlier). Measured for the Goldilocks sets; BabyBear's 48 MB key stays in L2,
@@ -1054,17 +1098,17 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
           }
         }
         NT::forward_small(x, xbuf, ping, s_tw, t, sync);
-        if (fold_due<F>(nprod)) {
+        if (fold_due_n<FA::FOLD>(nprod)) {
 #pragma unroll
           for (int v = 0; v < V; ++v) {
-            F::acc_fold(ax[v]);
-            F::acc_fold(ay[v]);
+            FA::fold(ax[v]);
+            FA::fold(ay[v]);
           }
         }
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          F::acc_mac(ax[v], x[v], k[v * T + t]);
-          F::acc_mac(ay[v], x[v], k[N + v * T + t]);
+          FA::mac(ax[v], x[v], k[v * T + t]);
+          FA::mac(ay[v], x[v], k[N + v * T + t]);
         }
         ++nprod;
       }
@@ -1073,11 +1117,57 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         const W off = ks ? off_ks : off_br;
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-          xbuf[v * T + t] = F::acc_value(ax[v], off);
-          xbuf[N + v * T + t] = F::acc_value(ay[v], off);
+          xbuf[v * T + t] = FA::value(ax[v], off);
+          xbuf[N + v * T + t] = FA::value(ay[v], off);
         }
       }
       __syncthreads();
+      if constexpr (TERN) {
+        if (!ks) {
+          // the half's polynomial: both pairs' sums (groups [0, D/2) and [D/2, D)) in its layout
+          W f0[VW], f1[VW];
+#pragma unroll
+          for (int vw = 0; vw < VW; ++vw) {
+            const int slot = tw * VW + vw;
+            const int at = half * N + (slot % V) * T + slot / V;
+            W s0 = s_x[at], s1 = s_x[(D / 2) * 2 * N + at];
+#pragma unroll 1
+            for (int h = 1; h < D / 2; ++h) {
+              s0 = F::add(s0, s_x[h * 2 * N + at]);
+              s1 = F::add(s1, s_x[(D / 2 + h) * 2 * N + at]);
+            }
+            f0[vw] = s0;
+            f1[vw] = s1;
+          }
+          __syncthreads();  // every partial read: the group buffers are free
+          // INTT(pair-1 sum) to a stage in group 1's buffer (the halves' exchange buffers are E's
+          // and group 0's), then INTT(pair-0 sum) in registers
+          W *st = s_x + 2 * N + half * N;
+          NW::inverse(f1, wbuf, ping_w, s_itw_w, tw, wsync);
+#pragma unroll
+          for (int vw = 0; vw < VW; ++vw) st[NW::natural_pos(tw, vw)] = F::canon(f1[vw]);
+          NW::inverse(f0, wbuf, ping_w, s_itw_w, tw, wsync);
+          wsync();  // the stage is complete
+          W *y = half == 0 ? acc_a : acc_b;
+          const int dr = (int)two_n - (int)ms[ph];
+#pragma unroll
+          for (int vw = 0; vw < VW; ++vw) {
+            const int k = NW::natural_pos(tw, vw);
+            const int sidx = k - dr;
+            W rot;
+            if (sidx >= 0) {
+              rot = st[sidx];
+            } else if (sidx >= -N) {
+              rot = F::neg_ref(st[sidx + N]);
+            } else {
+              rot = st[sidx + 2 * N];
+            }
+            y[k] = F::add(y[k], F::sub(F::canon(f0[vw]), rot));
+          }
+          __syncthreads();
+          continue;
+        }
+      }
       {
         // the half's sum over all groups' partials, read in its own layout: slot tw*VW + vw sits at
         // (slot % V) * T + slot / V in a group's buffer

@@ -1,7 +1,7 @@
 """Launches of at most one gate per SM take the latency form (bootstrap_dp_kernel: one gate per
 CTA, the gadget digits spread over the CTA's thread groups). Bit-exact against the oracle for every
 field and both key layouts (T = 64 and 128 threads per group), including ZAMA's 26 digits over 4
-groups and a launch of exactly one gate per SM."""
+groups, a launch of exactly one gate per SM, and ternary LWE keys."""
 
 import ctypes
 
@@ -77,5 +77,40 @@ def test_latency_form_goldilocks_cluster_and_single_sm(hb, oracle, oracle_keys, 
         k = oracle_keys(1)
         pick = sorted({0, count // 2, count - 1})
         assert (out[pick] == oracle.gate(k, "nand", c0[pick], c1[pick])).all()
+    finally:
+        ev.keys.free()
+
+
+@pytest.mark.parametrize("base", [3, 4])
+@pytest.mark.parametrize("T", [64, 128])
+def test_latency_form_ternary_lwe_key(hb, oracle, ctx, base, T):
+    """Ternary LWE keys in the latency form (one CTA per gate; the CTA's two halves of groups take
+    RGSW(s_i = 1) and RGSW(s_i = -1)) against the oracle's ternary blind rotation, over
+    DefaultFieldU32 with n = N (DEFAULT_TERNARY) and with two key-switching chunks
+    (CUSTOM_TERNARY), both key layouts; the plain one-group form gives the same words."""
+    from hasteboots_b200._lib import check, lib
+    from gpu_util import empty_dev, from_dev, to_dev
+    params = hb.Parameters.preset(base).with_ternary_lwe_key()
+    sk = hb.KeyGen.generate_secret_key(params, 0)
+    ev = hb.Evaluator(sk, ctx)
+    try:
+        check(lib().hb_keys_set_config(ctx.handle, ev.keys.handle, T, 4), "set_config", ctx.handle)
+        op = oracle.preset(base)
+        op.lwe_ternary = 1
+        k = oracle.keygen(op, 0)
+        bits = np.random.default_rng(90 + base).integers(0, 2, (3, 6)).astype(np.uint8)
+        c = [sk.encrypt(bits[i], 600 + 10 * i) for i in range(3)]
+        for g in ("nand", "xnor", "majority"):
+            if g == "majority":
+                out, ref = ev.majority(*c), oracle.gate(k, g, *c)
+            else:
+                out, ref = getattr(ev, g)(c[0], c[1]), oracle.gate(k, g, c[0], c[1])
+            assert (out == ref).all(), g
+        d0, d1 = to_dev(c[0]), to_dev(c[1])
+        dp = empty_dev(c[0].shape, c[0].dtype)
+        check(lib().hb_gate_device_plain(ctx.handle, ev.keys.handle, 0, d0.data_ptr(), d1.data_ptr(),
+                                         dp.data_ptr(), len(c[0])), "plain", ctx.handle)
+        ctx.synchronize()
+        assert (from_dev(dp, c[0].dtype) == ev.nand(c[0], c[1])).all()
     finally:
         ev.keys.free()
