@@ -660,7 +660,9 @@ int default_threads_per_gate(int field_id) {
 int default_gates_per_cta(int field_id) {
   const char *env = getenv("HB_GATES_PER_CTA");
   if (env && atoi(env) > 0) return atoi(env);
-  return field_id == HB_FIELD_GOLDILOCKS ? 4 : 6;
+  // measured best on B200 before autotuning: Goldilocks (T = 128) 4, BabyBear (T = 64, paired
+  // digit transforms) 8, DefaultFieldU32 (T = 64) 6
+  return field_id == HB_FIELD_GOLDILOCKS ? 4 : field_id == HB_FIELD_BABYBEAR ? 8 : 6;
 }
 
 }  // namespace

@@ -481,6 +481,20 @@ struct BootParams {
 #define HB_BOOT_PINGPONG 1
 #endif
 constexpr bool kBootPingPong = HB_BOOT_PINGPONG != 0;
+// Digit pairs: a bootstrap kernel variant that transforms two digits at once (GroupNtt::
+// forward_small2) gives each thread two independent transforms to interleave. Measured on B200
+// (16384 gates per launch), it pays for BabyBear where the launch leaves 128 registers per thread
+// (T G = 512 threads: T = 64, G = 8: 439.4 -> 427.7 ms; T = 128, G = 4: 501.7 -> 487.0 ms) and
+// costs elsewhere (BabyBear T = 64, G = 6: 447.9 -> 460.1 ms; DefaultFieldU32, whose 64-bit sums
+// already hold 32 more registers: up to 23 % slower), so only those variants use it.
+template <class F, int T, int G>
+__host__ __device__ constexpr bool boot_dual() {
+  if constexpr (sizeof(typename F::W) == 4) {
+    return !F::WIDE && T * G >= 512;
+  } else {
+    return false;
+  }
+}
 constexpr int kBootXbuf = kBootPingPong ? 2 : 1;  // exchange buffers of N words per gate
 
 template <class W, int N, int G, int S>
@@ -692,21 +706,9 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
       const uint32_t L = ks ? p.ks_len : p.len;
       const uint32_t bits = ks ? p.ks_bits : p.bits;
       const uint64_t mask = (1ULL << bits) - 1;
-      for (uint32_t j = 0; j < L; ++j) {
-        W x[V];
-        if (active) {
-          const uint32_t sh = j * bits;
-          digits<W, V, T>(x, ebuf, t, sh, (uint32_t)mask);
-          if constexpr (TRACE) {
-            // digit j of E.part at step ph / 2: coefficient v T + t is in x[v]
-            if (!ks && p.digits) {
-              uint8_t *dd = p.digits + ((((size_t)gate * n + (ph >> 1)) * 2 + part) * p.len + j) * N;
-#pragma unroll
-              for (int v = 0; v < V; ++v) dd[v * T + t] = (uint8_t)x[v];
-            }
-          }
-          NT::forward_small(x, xbuf, ping, s_tw, t, sync);
-        }
+      // multiply-accumulate of one transformed digit against its key chunk(s): false when the
+      // launch must stop
+      auto mac_digit = [&](W(&x)[V]) -> bool {
         const W *k = pipe.acquire();
         if (active) {
           if (fold_due<F>(nprod)) {
@@ -727,7 +729,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
           }
         }
         ++nprod;
-        if (!pipe.release(src, t, sync)) goto aborted;
+        if (!pipe.release(src, t, sync)) return false;
         if constexpr (TERN) {
           if (!ks) {  // the same digit against RGSW(s_i == -1)
             const W *k1 = pipe.acquire();
@@ -738,9 +740,44 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
                 F::acc_mac(acc_y1[v], x[v], k1[N + v * T + t]);
               }
             }
-            if (!pipe.release(src, t, sync)) goto aborted;
+            if (!pipe.release(src, t, sync)) return false;
           }
         }
+        return true;
+      };
+      // TRACE: digit j of E.part at step ph / 2; coefficient v T + t is in x[v]
+      auto trace_digit = [&](const W(&x)[V], uint32_t j) {
+        if constexpr (TRACE) {
+          if (!ks && p.digits) {
+            uint8_t *dd = p.digits + ((((size_t)gate * n + (ph >> 1)) * 2 + part) * p.len + j) * N;
+#pragma unroll
+            for (int v = 0; v < V; ++v) dd[v * T + t] = (uint8_t)x[v];
+          }
+        }
+      };
+      constexpr bool DUAL = boot_dual<F, T, G>();
+      uint32_t j = 0;
+      if constexpr (DUAL) {
+        for (; j + 1 < L; j += 2) {
+          W x[V], y[V];
+          if (active) {
+            digits<W, V, T>(x, ebuf, t, j * bits, (uint32_t)mask);
+            digits<W, V, T>(y, ebuf, t, (j + 1) * bits, (uint32_t)mask);
+            trace_digit(x, j);
+            trace_digit(y, j + 1);
+            NT::forward_small2(x, y, xbuf, ping, s_tw, t, sync);
+          }
+          if (!mac_digit(x) || !mac_digit(y)) goto aborted;
+        }
+      }
+      for (; j < L; ++j) {
+        W x[V];
+        if (active) {
+          digits<W, V, T>(x, ebuf, t, j * bits, (uint32_t)mask);
+          trace_digit(x, j);
+          NT::forward_small(x, xbuf, ping, s_tw, t, sync);
+        }
+        if (!mac_digit(x)) goto aborted;
       }
       if (KSC ? (ks ? ph + 1 < phases : part == 0) : (part == 0 && !ks)) continue;
       if constexpr (TERN) {

@@ -286,6 +286,35 @@ struct GroupNtt {
     }
   }
 
+  // Two independent forward transforms advanced pass by pass, so that the compiler can interleave
+  // their instructions between the exchanges (each exchange of each transform as in fwd_pass).
+  template <int TOP, bool SMALL>
+  __device__ __forceinline__ static void fwd_pass2(W (&x)[V], W (&y)[V], W *buf, int &ping, const W *tw, int t,
+                                                   const GroupSync<T> &sync) {
+    constexpr int LO = TOP - LOGV > 0 ? TOP - LOGV : 0;
+    if constexpr (R8 && TOP < LOGN && TOP - LO == 3) {
+      fwd_r8<LO, LOGN - TOP>(x, tw, t);
+      fwd_r8<LO, LOGN - TOP>(y, tw, t);
+    } else {
+      fwd_stages<TOP, TOP - 1, SMALL>(x, tw, t);
+      fwd_stages<TOP, TOP - 1, SMALL>(y, tw, t);
+    }
+    if constexpr (LO > 0) {
+      constexpr int NEXT = LO - LOGV > 0 ? LO - LOGV : 0;
+      static_assert(PP, "paired transforms use the two exchange buffers in turn");
+      exchange<LO, NEXT>(x, buf + ping * N, t, sync);
+      ping ^= 1;
+      exchange<LO, NEXT>(y, buf + ping * N, t, sync);
+      ping ^= 1;
+      fwd_pass2<LO, false>(x, y, buf, ping, tw, t, sync);
+    }
+  }
+  // forward_small of two digit polynomials at once.
+  __device__ __forceinline__ static void forward_small2(W (&x)[V], W (&y)[V], W *buf, int &ping, const W *tw,
+                                                        int t, const GroupSync<T> &sync) {
+    fwd_pass2<LOGN, true>(x, y, buf, ping, tw, t, sync);
+  }
+
   // x: natural-order values at natural_pos(t, v) -> slots at slot_pos(t, v).
   // buf: the group's exchange buffers (2 N words with PP, else N).
   __device__ __forceinline__ static void forward(W (&x)[V], W *buf, int &ping, const W *tw, int t,
