@@ -544,16 +544,31 @@ def extra_legs(args):
     """The other configurations, measured after the headline in the default run (about a minute):
     config 1 (single BABYBEAR NAND), 2 (NTT / external-product microbench), 4 (the mixed-set graph
     against the same jobs back to back) and 5 (a shortened serving run with load shedding)."""
-    sets = KeySets()
-    sk, ev = sets.evs[0]
-    out = {"single": leg_single(sets.ctx, sk, ev, 20, 3),
-           "ntt_microbench": leg_ntt(sets.ctx, 5, 2),
-           "mixed": leg_mixed(sets, 2, 1, load_json("tests", "golden", "digests_full.json")),
-           "serve": leg_serve(sets, args.extra_serve_s, 200.0, 10.0, 2.0)}
+    legs = {
+        "single": lambda: leg_single(sets.ctx, sets.evs[0][0], sets.evs[0][1], 20, 3),
+        "ntt_microbench": lambda: leg_ntt(sets.ctx, 5, 2),
+        "mixed": lambda: leg_mixed(sets, 2, 1, load_json("tests", "golden", "digests_full.json")),
+        "serve": lambda: leg_serve(sets, args.extra_serve_s, 200.0, 10.0, 2.0),
+    }
+    passed = {
+        "single": lambda r: all(r["checks"].values()),
+        "ntt_microbench": lambda r: r["checks"]["roundtrips_exact"],
+        "mixed": lambda r: r["checks"]["truth_tables"] and r["checks"]["oracle_digest_match"] is not False,
+        "serve": lambda r: r["checks"]["served_equals_alone"],
+    }
+    out, ok = {}, True
+    try:
+        sets = KeySets()
+    except Exception as e:  # the headline line is printed with the error in place of the legs
+        return {"extras_error": repr(e)}, False
+    for name, leg in legs.items():
+        try:
+            out[name] = leg()
+            ok = ok and bool(passed[name](out[name]))
+        except Exception as e:
+            out[name] = {"error": repr(e)}
+            ok = False
     sets.close()
-    ok = (all(out["single"]["checks"].values()) and out["ntt_microbench"]["checks"]["roundtrips_exact"]
-          and out["mixed"]["checks"]["truth_tables"] and out["mixed"]["checks"]["oracle_digest_match"] is not False
-          and out["serve"]["checks"]["served_equals_alone"])
     return out, ok
 
 
