@@ -50,3 +50,18 @@ def test_every_entry_point_refuses_null_arguments(hb):
             assert rc == 0, name
         else:
             assert _lib.ERRORS.get(rc) == "HB_ERR_INVALID", (name, rc)
+
+
+def test_c_client_compiles_and_links():
+    """A C caller builds against include/hb_gpu.h and links libhb_gpu.so (tests/c_client; run by
+    tests/test_gpu_c_client.py on a GPU)."""
+    import subprocess
+    import tempfile
+    from hasteboots_b200 import build
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(tempfile.mkdtemp(), "nand_client")
+    libdir = os.path.dirname(build.OUT)
+    subprocess.run(["gcc", "-O2", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "c_client", "nand_client.c"), "-o", exe,
+                    "-L", libdir, "-lhb_gpu", "-Wl,-rpath," + libdir], check=True)
+    assert os.path.exists(exe)
