@@ -477,7 +477,7 @@ def leg_single(ctx, sk, ev, steps, warmup):
     import torch
     from hasteboots_b200._lib import check, lib
     params = sk.params
-    c0, c1 = sk.encrypt([1], 0), sk.encrypt([1], 1)
+    c0, c1 = sk.encrypt([1], 0), sk.encrypt([1], 1)  # NAND(1, 1) = 0
     ivt = _ivt(params)
     d0 = torch.from_numpy(c0.view(ivt).copy()).cuda()
     d1 = torch.from_numpy(c1.view(ivt).copy()).cuda()
@@ -515,6 +515,8 @@ def run_workload(args):
     base = {"n_gpus": 1, "data": "synthetic (seed-0 keys)"}
     if args.workload == "single":
         params = tfhe.Parameters.preset(args.single_preset)
+        if args.ternary_lwe_key:
+            params = params.with_ternary_lwe_key()
         sk = tfhe.KeyGen.generate_secret_key(params, 0)
         ctx = tfhe.Context(0)
         ev = tfhe.Evaluator(sk, ctx)
@@ -592,6 +594,8 @@ def main():
                          "3 DEFAULT_TERNARY, 4 CUSTOM_TERNARY")
     ap.add_argument("--single-preset", type=int, default=0,
                     help="single: the parameter set of the one gate (default 0, BABYBEAR)")
+    ap.add_argument("--ternary-lwe-key", action="store_true",
+                    help="single: a ternary LWE key (DefaultFieldU32 presets 3 and 4 only)")
     ap.add_argument("--workload", default="gates", choices=["gates", "mixed", "ntt", "single", "serve"],
                     help="gates: 16384 NAND gates (default, the contract line); mixed: 64 jobs across "
                          "the three sets in one graph; ntt: NTT/external-product microbench; single: "
