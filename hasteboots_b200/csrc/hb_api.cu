@@ -239,15 +239,20 @@ uint32_t ks_dim(const hb_params &p) {
 }
 
 // Twiddle tables of the half-CTA groups of bootstrap_dp_kernel for keys laid out for T threads
-// (words per thread of those groups: hb::dp_wide_words).
+// (words per thread of those groups: hb::dp_wide_words), for one CTA per gate and for the cluster
+// form (the 32-bit fields' cluster CTAs hold half as many groups).
 int dp_tables(hb_ctx *ctx, const hb_params &p, int T) {
   if (p.ring_dim != 1024) return HB_OK;
   const int ws = p.field_id == HB_FIELD_GOLDILOCKS ? 8 : 4;
-  const int D = ws == 8 ? 4 : 512 / T, vw = 1024 / (D / 2 * T);
-  uint32_t logv = 0;
-  while ((1 << logv) < vw) ++logv;
-  DevTables *tb;
-  return tables(ctx, p.field_id, 10, &tb, logv);
+  for (int cl = 0; cl < 2; ++cl) {
+    const int D = ws == 8 ? 4 : (cl ? 256 : 512) / T, vw = 1024 / (D / 2 * T);
+    uint32_t logv = 0;
+    while ((1 << logv) < vw) ++logv;
+    DevTables *tb;
+    const int rc = tables(ctx, p.field_id, 10, &tb, logv);
+    if (rc) return rc;
+  }
+  return HB_OK;
 }
 
 // Device words of the key-switching key: every n'-word chunk key polynomial spread to N words.
@@ -411,15 +416,18 @@ GateJob make_job(uint64_t P, int gate, uint32_t N, const void *c0, const void *c
 
 
 // Launches of at most one gate per SM (G = 1 outside the plain form) run the latency form: one gate
-// per CTA, its digits spread over the CTA's thread groups (binary LWE keys);
-// for the Goldilocks sets, whose 2l digits outnumber one CTA's groups, a cluster of kDpCluster CTAs
-// per gate while the whole launch fits the GPU's co-resident clusters.
-constexpr int kDpCluster = 4;
+// per CTA, its digits spread over the CTA's thread groups. With a binary LWE key a gate takes a
+// cluster of CTAs instead while the launch holds at most one cluster CTA per SM: kDpCluster64 CTAs
+// of 4 groups for the Goldilocks sets (2l = 16 digits), kDpCluster32 CTAs of 256 threads for the
+// 32-bit fields (BabyBear's 2l = 8 digits one per group), so that each SM transforms a share of a
+// step's digits and every CTA inverse-transforms the summed a and b polynomials itself.
+constexpr int kDpCluster64 = 4;
+constexpr int kDpCluster32 = 2;
 
 template <class F, int LOGN, int T, int C, bool KSC, bool TERN = false>
 int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream, int *max_clusters) {
   using W = typename F::W;
-  constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T>();
+  constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T, C>();
   auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D, C, KSC, TERN>;
   const size_t smem = hb::dp_smem_bytes<W, N, D, C>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -456,25 +464,33 @@ int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStrea
   return HB_OK;
 }
 
+// Inverse twiddles of the half-CTA groups of the latency form with C CTAs per gate; built with the
+// keys (hb_keys_upload / hb_keys_generate / relayout), never inside a capture.
+template <class F, int LOGN, int T, int C>
+const typename F::W *dp_wide_itw(hb_ctx *ctx) {
+  constexpr int LOGVW = hb::ilog2c(hb::dp_wide_words<typename F::W, 1 << LOGN, T, C>());
+  return (const typename F::W *)ctx->tables[F::FIELD_ID][LOGN][LOGVW].itw;
+}
+
 template <class F, int LOGN, int T, bool KSC, bool TERN = false>
 int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t stream) {
   using W = typename F::W;
-  constexpr int N = 1 << LOGN;
-  constexpr int LOGVW = hb::ilog2c(hb::dp_wide_words<W, N, T>());
-  // built with the keys (hb_keys_upload / hb_keys_generate / relayout), never inside a capture
-  const DevTables &tbw = ctx->tables[F::FIELD_ID][LOGN][LOGVW];
-  if (!tbw.itw) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
-  prm.itw_w = (const W *)tbw.itw;
-  if constexpr (sizeof(W) == 8 && !TERN) {
-    std::atomic<int> &cached = ctx->dp_clusters[T == 128 ? 1 : 0];
+  constexpr int CL = sizeof(W) == 8 ? kDpCluster64 : kDpCluster32;
+  if constexpr (!TERN) {
+    std::atomic<int> &cached = ctx->dp_clusters[(sizeof(W) == 8 ? 0 : 2) + (T == 128 ? 1 : 0)];
     int m = cached.load();
+    prm.itw_w = dp_wide_itw<F, LOGN, T, CL>(ctx);
+    if (!prm.itw_w) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
     if (m < 0) {  // the same shared memory and threads with or without KSC
-      const int rc = launch_dp_c<F, LOGN, T, kDpCluster, KSC>(ctx, prm, stream, &m);
+      const int rc = launch_dp_c<F, LOGN, T, CL, KSC>(ctx, prm, stream, &m);
       if (rc) return rc;
+      m = std::min(m, ctx->sms / CL);  // one cluster CTA per SM
       cached.store(m);
     }
-    if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, kDpCluster, KSC>(ctx, prm, stream, nullptr);
+    if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, CL, KSC>(ctx, prm, stream, nullptr);
   }
+  prm.itw_w = dp_wide_itw<F, LOGN, T, 1>(ctx);
+  if (!prm.itw_w) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
   return launch_dp_c<F, LOGN, T, 1, KSC, TERN>(ctx, prm, stream, nullptr);
 }
 

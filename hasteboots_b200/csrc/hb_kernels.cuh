@@ -896,18 +896,20 @@ aborted:
 // Latency form: one gate per CTA, its gadget digits spread over D thread groups
 // ------------------------------------------------------------------------------------------
 
-// Groups per CTA of bootstrap_dp_kernel: as many T-thread groups as 512 threads hold (the 64-bit
-// transforms keep about 128 registers a thread, so 4 groups of 128 or of 64).
-template <class W, int T>
+// Groups per CTA of bootstrap_dp_kernel with C CTAs per gate: as many T-thread groups as 512
+// threads hold (the 64-bit transforms keep about 128 registers a thread, so 4 groups of 128 or of
+// 64); a 32-bit field's cluster CTA holds half as many (256 threads), so that BabyBear's 2l = 8
+// digits still give every group of a 2-CTA cluster one digit.
+template <class W, int T, int C = 1>
 __host__ __device__ constexpr int dp_groups() {
-  return sizeof(W) == 8 ? 4 : 512 / T;
+  return sizeof(W) == 8 ? 4 : (C > 1 ? 256 : 512) / T;
 }
 
 // Words per thread of the half-CTA groups (D/2 groups of T threads) that sum and inverse-transform
 // the a and b polynomials in bootstrap_dp_kernel.
-template <class W, int N, int T>
+template <class W, int N, int T, int C = 1>
 __host__ __device__ constexpr int dp_wide_words() {
-  return N / (dp_groups<W, T>() / 2 * T);
+  return N / (dp_groups<W, T, C>() / 2 * T);
 }
 
 // Shared memory of bootstrap_dp_kernel: twiddles (3N words: forward, inverse, inverse of the

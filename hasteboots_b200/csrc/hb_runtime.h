@@ -44,9 +44,9 @@ struct hb_ctx {
   std::atomic<unsigned long long> launches{0};  // bootstrap kernel launches issued by this context
   long long wait_limit = 0;                     // SM clock cycles per bounded wait; 0 = default
   int withhold_keys = 0;                        // test hook: bootstrap launches issue no key copies
-  // co-resident latency-form clusters (Goldilocks, T = 64 / 128); -1 unknown. Atomic: the serving
-  // loop's worker thread launches on the context too.
-  std::atomic<int> dp_clusters[2] = {-1, -1};
+  // latency-form clusters the GPU holds with one cluster CTA per SM ([Goldilocks, 32-bit fields] x
+  // [T = 64, 128]); -1 unknown. Atomic: the serving loop's worker thread launches on the context too.
+  std::atomic<int> dp_clusters[4] = {-1, -1, -1, -1};
   // device address of the allocation-free MUX's in-library array, looked up by the first such call
   // on this context (a context made after a device reset looks it up again)
   void *noalloc_addr = nullptr;

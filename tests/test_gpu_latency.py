@@ -1,7 +1,8 @@
 """Launches of at most one gate per SM take the latency form (bootstrap_dp_kernel: one gate per
-CTA, the gadget digits spread over the CTA's thread groups). Bit-exact against the oracle for every
-field and both key layouts (T = 64 and 128 threads per group), including ZAMA's 26 digits over 4
-groups, a launch of exactly one gate per SM, and ternary LWE keys."""
+CTA, or a cluster of CTAs with a binary LWE key, the gadget digits spread over the thread groups).
+Bit-exact against the oracle for every field and both key layouts (T = 64 and 128 threads per
+group), including ZAMA's 26 digits over 4 groups, launches at the cluster limit and one gate past
+it, a launch of exactly one gate per SM, and ternary LWE keys."""
 
 import ctypes
 
@@ -63,18 +64,19 @@ def test_latency_form_one_gate_per_sm(hb, oracle, oracle_keys, ctx):
         ev.keys.free()
 
 
-@pytest.mark.parametrize("count", [3, 100])
-def test_latency_form_goldilocks_cluster_and_single_sm(hb, oracle, oracle_keys, ctx, count):
-    """Goldilocks launches small enough for a cluster of CTAs per gate (3 gates) and beyond the
-    GPU's co-resident clusters (100 gates: one SM per gate) against the oracle."""
-    sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(1), 0)
+@pytest.mark.parametrize("pid,count", [(1, 3), (1, 37), (1, 100), (0, 1), (0, 74), (0, 75), (4, 5), (3, 2)])
+def test_latency_form_cluster_and_single_sm(hb, oracle, oracle_keys, ctx, pid, count):
+    """Launches small enough for a cluster of CTAs per gate (Goldilocks: 4 CTAs, up to 37 gates on
+    148 SMs; 32-bit fields: 2 CTAs, up to 74 gates, CUSTOM_TERNARY with its two key-switching
+    chunks) and just beyond (one SM per gate) against the oracle."""
+    sk = hb.KeyGen.generate_secret_key(hb.Parameters.preset(pid), 0)
     ev = hb.Evaluator(sk, ctx)
     try:
         bits = np.random.default_rng(70 + count).integers(0, 2, (2, count)).astype(np.uint8)
         c0, c1 = sk.encrypt(bits[0], 7000), sk.encrypt(bits[1], 8000)
         out = ev.nand(c0, c1)
         assert (sk.decrypt(out) == 1 - (bits[0] & bits[1])).all()
-        k = oracle_keys(1)
+        k = oracle_keys(pid)
         pick = sorted({0, count // 2, count - 1})
         assert (out[pick] == oracle.gate(k, "nand", c0[pick], c1[pick])).all()
     finally:
