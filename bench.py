@@ -471,9 +471,10 @@ def leg_serve(sets, duration, rate, drain, max_queue_s):
 
 
 def leg_single(ctx, sk, ev, steps, warmup):
-    """Config 1: latency of one NAND gate through hb_gate_device (the latency form: one CTA -- for
-    the Goldilocks sets a cluster of CTAs -- whose thread groups share the gate's digits), with the
-    plain form (one kernel launch of a single thread group) beside it."""
+    """Config 1: latency of one NAND gate through hb_gate_device (the latency form: a cluster of
+    CTAs -- 4 for the Goldilocks sets, 2 for the 32-bit fields; one CTA with a ternary LWE key --
+    whose thread groups share the gate's digits), with the plain form (one kernel launch of a single
+    thread group) beside it."""
     import torch
     from hasteboots_b200._lib import check, lib
     params = sk.params
@@ -503,8 +504,9 @@ def leg_single(ctx, sk, ev, steps, warmup):
             "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
             "plain_form_ms": {"p50": float(np.percentile(ptimes, 50)), "p99": float(np.percentile(ptimes, 99))},
             "config": {"workload": "1 NAND gate through hb_gate_device (the latency form: the gate's digits "
-                                   "over the thread groups of one CTA, or of a 4-CTA cluster for the "
-                                   "Goldilocks sets); plain form: one launch of one thread group"},
+                                   "over the thread groups of a 4-CTA cluster for the Goldilocks sets, a "
+                                   "2-CTA cluster for the 32-bit fields, one CTA with a ternary LWE key); "
+                                   "plain form: one launch of one thread group"},
             "clocks": clk.summary(),
             "checks": {"nand(1,1)=0": bool(bit == 0), "equals_plain_form": same}}
 

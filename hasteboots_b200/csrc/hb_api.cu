@@ -238,19 +238,22 @@ uint32_t ks_dim(const hb_params &p) {
   return m;
 }
 
-// Twiddle tables of the half-CTA groups of bootstrap_dp_kernel for keys laid out for T threads
-// (words per thread of those groups: hb::dp_wide_words), for one CTA per gate and for the cluster
-// form (the 32-bit fields' cluster CTAs hold half as many groups).
+// Twiddle tables of bootstrap_dp_kernel for keys laid out for T threads, for one CTA per gate and
+// for the cluster form: those of its groups' digit transforms (hb::dp_group_threads) and of its
+// half-CTA groups (words per thread: hb::dp_wide_words).
 int dp_tables(hb_ctx *ctx, const hb_params &p, int T) {
   if (p.ring_dim != 1024) return HB_OK;
   const int ws = p.field_id == HB_FIELD_GOLDILOCKS ? 8 : 4;
   for (int cl = 0; cl < 2; ++cl) {
-    const int D = ws == 8 ? 4 : (cl ? 256 : 512) / T, vw = 1024 / (D / 2 * T);
-    uint32_t logv = 0;
-    while ((1 << logv) < vw) ++logv;
-    DevTables *tb;
-    const int rc = tables(ctx, p.field_id, 10, &tb, logv);
-    if (rc) return rc;
+    // hb::dp_group_threads, hb::dp_groups: the groups' own transforms and the half-CTA groups'
+    const int tg = ws == 4 && cl ? 128 : T, D = ws == 8 ? 4 : 512 / tg;
+    for (int words : {1024 / tg, 1024 / (D / 2 * tg)}) {
+      uint32_t logv = 0;
+      while ((1 << logv) < words) ++logv;
+      DevTables *tb;
+      const int rc = tables(ctx, p.field_id, 10, &tb, logv);
+      if (rc) return rc;
+    }
   }
   return HB_OK;
 }
@@ -418,23 +421,24 @@ GateJob make_job(uint64_t P, int gate, uint32_t N, const void *c0, const void *c
 // Launches of at most one gate per SM (G = 1 outside the plain form) run the latency form: one gate
 // per CTA, its digits spread over the CTA's thread groups. With a binary LWE key a gate takes a
 // cluster of CTAs instead while the launch holds at most one cluster CTA per SM: kDpCluster64 CTAs
-// of 4 groups for the Goldilocks sets (2l = 16 digits), kDpCluster32 CTAs of 256 threads for the
-// 32-bit fields (BabyBear's 2l = 8 digits one per group), so that each SM transforms a share of a
-// step's digits and every CTA inverse-transforms the summed a and b polynomials itself.
+// of 4 groups for the Goldilocks sets (2l = 16 digits), kDpCluster32 CTAs of 4 groups of 128
+// threads for the 32-bit fields (BabyBear's 2l = 8 digits one per group), so that each SM
+// transforms a share of a step's digits and every CTA inverse-transforms the summed a and b
+// polynomials itself.
 constexpr int kDpCluster64 = 4;
 constexpr int kDpCluster32 = 2;
 
-template <class F, int LOGN, int T, int C, bool KSC, bool TERN = false>
-int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream, int *max_clusters) {
+template <class F, int LOGN, int T, int C, bool KSC, bool TERN, bool KST>
+int launch_dp_k(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream, int *max_clusters) {
   using W = typename F::W;
-  constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T, C>();
-  auto kern = hb::bootstrap_dp_kernel<F, LOGN, T, D, C, KSC, TERN>;
-  const size_t smem = hb::dp_smem_bytes<W, N, D, C>(prm.n);
+  constexpr int N = 1 << LOGN, D = hb::dp_groups<W, T, C>(), TG = hb::dp_group_threads<W, T, C>();
+  auto kern = hb::bootstrap_dp_kernel<F, LOGN, TG, D, C, KSC, TERN, T, KST>;
+  const size_t smem = hb::dp_smem_bytes<W, N, D, C, KST>(prm.n);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "bootstrap smem attribute");
   if constexpr (C == 1) {
     const unsigned grid = std::max(1u, std::min<unsigned>(prm.total_batches, (unsigned)ctx->sms));
-    kern<<<grid, D * T, smem, stream>>>(prm);
+    kern<<<grid, D * TG, smem, stream>>>(prm);
   } else {
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
@@ -442,7 +446,7 @@ int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStrea
     attr[0].val.clusterDim.x = C;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.blockDim = dim3(D * T);
+    cfg.blockDim = dim3(D * TG);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cfg.attrs = attr;
@@ -464,12 +468,33 @@ int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStrea
   return HB_OK;
 }
 
-// Inverse twiddles of the half-CTA groups of the latency form with C CTAs per gate; built with the
-// keys (hb_keys_upload / hb_keys_generate / relayout), never inside a capture.
+// The latency form with C CTAs per gate. Key words staged through shared memory (KST) only for the
+// 32-bit fields' clusters whose groups take more than one digit per step (DEFAULT_TERNARY: 18
+// digits over 8 groups, one gate 10.75 -> 10.09 ms); a single digit per group (BABYBEAR,
+// CUSTOM_TERNARY) and the Goldilocks sets measured 4-7 % slower with it.
+template <class F, int LOGN, int T, int C, bool KSC, bool TERN = false>
+int launch_dp_c(hb_ctx *ctx, const hb::BootParams<typename F::W> &prm, cudaStream_t stream, int *max_clusters) {
+  using W = typename F::W;
+  if constexpr (sizeof(W) == 4 && C > 1 && !TERN) {
+    if (2 * prm.len > (uint32_t)(C * hb::dp_groups<W, T, C>()))
+      return launch_dp_k<F, LOGN, T, C, KSC, TERN, true>(ctx, prm, stream, max_clusters);
+  }
+  return launch_dp_k<F, LOGN, T, C, KSC, TERN, false>(ctx, prm, stream, max_clusters);
+}
+
+// Twiddles of the latency form with C CTAs per gate over keys laid out for T threads: those of the
+// groups' digit transforms and the half-CTA groups' inverse twiddles. Built with the keys
+// (hb_keys_upload / hb_keys_generate / relayout), never inside a capture; false if missing.
 template <class F, int LOGN, int T, int C>
-const typename F::W *dp_wide_itw(hb_ctx *ctx) {
-  constexpr int LOGVW = hb::ilog2c(hb::dp_wide_words<typename F::W, 1 << LOGN, T, C>());
-  return (const typename F::W *)ctx->tables[F::FIELD_ID][LOGN][LOGVW].itw;
+bool dp_twiddles(hb_ctx *ctx, hb::BootParams<typename F::W> &prm) {
+  using W = typename F::W;
+  constexpr int N = 1 << LOGN;
+  constexpr int LOGV = hb::ilog2c(N / hb::dp_group_threads<W, T, C>());
+  constexpr int LOGVW = hb::ilog2c(hb::dp_wide_words<W, N, T, C>());
+  prm.tw = (const W *)ctx->tables[F::FIELD_ID][LOGN][LOGV].tw;
+  prm.itw = (const W *)ctx->tables[F::FIELD_ID][LOGN][LOGV].itw;
+  prm.itw_w = (const W *)ctx->tables[F::FIELD_ID][LOGN][LOGVW].itw;
+  return prm.tw && prm.itw && prm.itw_w;
 }
 
 template <class F, int LOGN, int T, bool KSC, bool TERN = false>
@@ -479,18 +504,17 @@ int launch_dp(hb_ctx *ctx, hb::BootParams<typename F::W> prm, cudaStream_t strea
   if constexpr (!TERN) {
     std::atomic<int> &cached = ctx->dp_clusters[(sizeof(W) == 8 ? 0 : 2) + (T == 128 ? 1 : 0)];
     int m = cached.load();
-    prm.itw_w = dp_wide_itw<F, LOGN, T, CL>(ctx);
-    if (!prm.itw_w) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
+    hb::BootParams<W> cp = prm;
+    if (!dp_twiddles<F, LOGN, T, CL>(ctx, cp)) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
     if (m < 0) {  // the same shared memory and threads with or without KSC
-      const int rc = launch_dp_c<F, LOGN, T, CL, KSC>(ctx, prm, stream, &m);
+      const int rc = launch_dp_c<F, LOGN, T, CL, KSC>(ctx, cp, stream, &m);
       if (rc) return rc;
       m = std::min(m, ctx->sms / CL);  // one cluster CTA per SM
       cached.store(m);
     }
-    if (prm.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, CL, KSC>(ctx, prm, stream, nullptr);
+    if (cp.total_batches <= (uint32_t)m) return launch_dp_c<F, LOGN, T, CL, KSC>(ctx, cp, stream, nullptr);
   }
-  prm.itw_w = dp_wide_itw<F, LOGN, T, 1>(ctx);
-  if (!prm.itw_w) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
+  if (!dp_twiddles<F, LOGN, T, 1>(ctx, prm)) return fail(ctx, HB_ERR_INVALID, "keys were not prepared on this context");
   return launch_dp_c<F, LOGN, T, 1, KSC, TERN>(ctx, prm, stream, nullptr);
 }
 

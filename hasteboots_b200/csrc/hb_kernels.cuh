@@ -896,29 +896,37 @@ aborted:
 // Latency form: one gate per CTA, its gadget digits spread over D thread groups
 // ------------------------------------------------------------------------------------------
 
-// Groups per CTA of bootstrap_dp_kernel with C CTAs per gate: as many T-thread groups as 512
-// threads hold (the 64-bit transforms keep about 128 registers a thread, so 4 groups of 128 or of
-// 64); a 32-bit field's cluster CTA holds half as many (256 threads), so that BabyBear's 2l = 8
-// digits still give every group of a 2-CTA cluster one digit.
-template <class W, int T, int C = 1>
+// Threads per group of bootstrap_dp_kernel with C CTAs per gate, over keys laid out for KT threads:
+// the key layout's width, except in the 32-bit fields' cluster form, whose groups transform a digit
+// with 128 threads (a 64-thread key layout is then read in the 128-thread slot order), so that
+// BabyBear's 2l = 8 digits give each of the 2 x 4 groups of a 2-CTA cluster one digit.
+template <class W, int KT, int C = 1>
+__host__ __device__ constexpr int dp_group_threads() {
+  return sizeof(W) == 4 && C > 1 ? 128 : KT;
+}
+
+// Groups per CTA of bootstrap_dp_kernel: as many groups as 512 threads hold (the 64-bit transforms
+// keep about 128 registers a thread, so 4 groups of 128 or of 64).
+template <class W, int KT, int C = 1>
 __host__ __device__ constexpr int dp_groups() {
-  return sizeof(W) == 8 ? 4 : (C > 1 ? 256 : 512) / T;
+  return sizeof(W) == 8 ? 4 : 512 / dp_group_threads<W, KT, C>();
 }
 
-// Words per thread of the half-CTA groups (D/2 groups of T threads) that sum and inverse-transform
-// the a and b polynomials in bootstrap_dp_kernel.
-template <class W, int N, int T, int C = 1>
+// Words per thread of the half-CTA groups (D/2 groups) that sum and inverse-transform the a and b
+// polynomials in bootstrap_dp_kernel.
+template <class W, int N, int KT, int C = 1>
 __host__ __device__ constexpr int dp_wide_words() {
-  return N / (dp_groups<W, T, C>() / 2 * T);
+  return N / (dp_groups<W, KT, C>() / 2 * dp_group_threads<W, KT, C>());
 }
 
-// Shared memory of bootstrap_dp_kernel: twiddles (3N words: forward, inverse, inverse of the
-// half-CTA layout), the accumulator (2N), the decomposition sources E.a and E.b (2N), per group
-// two exchange buffers (2N) that also carry the group's partial sums, in a cluster two buffers of
-// the CTA's partial sums that the other CTAs read (2 x 2N), and the modulus-switched input.
-template <class W, int N, int D, int C>
+// Shared memory of bootstrap_dp_kernel: twiddles (2N words: forward, inverse of the half-CTA
+// layout), the accumulator (2N), the decomposition sources E.a and E.b (2N), per group two exchange
+// buffers (2N) that also carry the group's partial sums, with KST the key words of its digit (2N), in a
+// cluster two buffers of the CTA's partial sums that the other CTAs read (2 x 2N), and the
+// modulus-switched input.
+template <class W, int N, int D, int C, bool KST>
 __host__ __device__ constexpr size_t dp_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(7 + 2 * D + (C > 1 ? 4 : 0)) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
+  return sizeof(W) * (size_t)(6 + (KST ? 4 : 2) * D + (C > 1 ? 4 : 0)) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
 }
 
 // Cluster barrier halves (all threads of every CTA of the cluster, warp-uniform): arrive releases
@@ -941,11 +949,14 @@ __device__ __forceinline__ const W *cluster_peer(const W *p, uint32_t rank) {
 // The same bootstrap as bootstrap_kernel (binary LWE key, one key-switching chunk) with the
 // latency of one gate cut instead of the cost of many: per blind-rotation step the 2l digit
 // polynomials of E = ACC (X^r - 1) go to D groups (digit d to group d mod D), each transforms its
-// digits and multiply-accumulates them with their key rows read straight from global memory
-// (no staging, no waits), the groups' partial sums meet in shared memory, and the two halves of
-// the CTA, each one group of D/2 * T threads, inverse-transform the a and b sums and add them to
-// the accumulator. The key switch spreads its
-// l_ks digits the same way. Used for launches of at most one gate per SM.
+// digits and multiply-accumulates them with their key rows, the groups' partial sums meet in shared
+// memory, and the two halves of the CTA, each one group of D/2 * T threads, inverse-transform the
+// a and b sums and add them to the accumulator. The key switch spreads its l_ks digits the same
+// way. Used for launches of at most one gate per SM.
+//
+// KST: every thread copies its key words of a digit into shared memory (cp.async) before the
+// digit's transform and waits for them after it; otherwise the key words are read from global
+// memory after the transform (with an L2 prefetch before it for the 64-bit keys, which exceed L2).
 //
 // C > 1: a cluster of C CTAs (C SMs) per gate. The digits go to the C * D groups of the cluster;
 // each CTA sums its groups' partials, the CTAs read each other's sums through distributed shared
@@ -959,45 +970,53 @@ __device__ __forceinline__ const W *cluster_peer(const W *p, uint32_t rank) {
 // the key-switch phase is digit d mod l_ks of chunk d / l_ks, whose source words are formed from
 // the accumulator where the digit is taken, and the extraction reads every (N/n')-th coefficient.
 //
+// KT < T: the key rows are laid out for KT-thread groups (word v KT + t' holds slot t' (N/KT) + v);
+// a group of T threads reads the same slots in its own order.
+//
 // TERN (ternary LWE key, one CTA per gate): in a blind-rotation step the first half of the groups
 // multiplies all 2l digits by RGSW(s_i == 1), the second half by RGSW(s_i == -1), so no group
 // holds two sets of sums. Each CTA half then reads both pairs' sums of its polynomial,
 // inverse-transforms the pair-1 sum into a stage and the pair-0 sum in registers, and adds
 // INTT(pair-0 sum) - X^(2N - a_i) INTT(pair-1 sum) to the accumulator: the evaluation key
 // RGSW_0 + RGSW_1 (-X^-a_i) of bootstrap_kernel's TERN step (ternary.rs:78-114).
-template <class F, int LOGN, int T, int D, int C = 1, bool KSC = false, bool TERN = false>
+template <class F, int LOGN, int T, int D, int C = 1, bool KSC = false, bool TERN = false, int KT = T,
+          bool KST = false>
 __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T>;
   constexpr int N = 1 << LOGN, V = NT::V, NT_ALL = D * T;
   static_assert(D >= 2 && D % 2 == 0, "two half-CTA groups transform the a and b sums");
   static_assert(!TERN || (C == 1 && D >= 4), "ternary keys: one CTA per gate, a pair per CTA half");
+  static_assert(KT <= T && T % KT == 0, "a group reads a key layout of at most its own width");
   constexpr int TW = D / 2 * T;  // threads of a half-CTA group
   using NW = GroupNtt<F, LOGN, TW>;
   constexpr int VW = NW::V;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_itw = s_tw + N;
-  W *s_itw_w = s_itw + N;
+  W *s_itw_w = s_tw + N;
   W *acc_a = s_itw_w + N;
   W *acc_b = acc_a + N;
   W *s_e = acc_b + N;  // E.a then E.b (the key switch: -acc.a), natural order
   W *s_x = s_e + 2 * N;
-  W *s_cp = s_x + D * 2 * N;  // C > 1: this CTA's partial sums (a then b) x 2, read by the cluster
+  W *s_k = s_x + D * 2 * N;  // KST, per group: its digit's key words at (v T + t) and N + (v T + t)
+  W *s_cp = s_k + (KST ? D * 2 * N : 0);  // C > 1: this CTA's partial sums (a then b) x 2, read by the cluster
   uint16_t *ms = reinterpret_cast<uint16_t *>(s_cp + (C > 1 ? 4 * N : 0));
 
   const int tid = threadIdx.x, g = tid / T, t = tid % T;
+  // key word of the group's (t, v): slot t V + v sits at (slot % (N/KT)) KT + slot / (N/KT)
+  constexpr int KM = T / KT;
+  const int kbase = (t % KM) * V * KT + t / KM;
   const uint32_t rank = C > 1 ? cluster_rank() : 0;
   const int gg = (int)rank * D + g;  // the group's index in the cluster (digits gg, gg + C D, ...)
   uint32_t cp_turn = 0;              // C > 1: which sum buffer this phase writes
   for (int i = tid; i < N; i += NT_ALL) {
     s_tw[i] = p.tw[i];
-    s_itw[i] = p.itw[i];
     s_itw_w[i] = p.itw_w[i];
   }
   __syncthreads();
   GroupSync<T> sync{1 + g};
   W *xbuf = s_x + g * 2 * N;
+  W *kbuf = s_k + g * 2 * N;
   int ping = 0;
   // half 0 (groups 0 .. D/2-1) sums and transforms the a polynomial, half 1 the b polynomial
   const int half = g / (D / 2), tw = tid % TW;
@@ -1099,6 +1118,28 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
       uint32_t nprod = 0;  // products in ax / ay since their last fold
       for (uint32_t d = ks ? (uint32_t)gg : br_first; d < nd; d += ks ? C * D : br_lanes) {
         const uint32_t part = ks ? 0 : d / L, j = ks ? d % p.ks_len : d % L;
+        const W *krow = ks     ? p.ksk + (size_t)d * 2 * N
+                        : TERN ? p.bsk + ((((size_t)ph * 2 + br_pair) * 2 + part) * L + j) * 2 * N
+                               : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
+        if constexpr (KST) {
+          // the thread's key words of this digit, copied to its own slots of the group's key stage
+          // while the digit is decomposed and transformed; the thread reads back only the words it
+          // copied, after its own wait
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            cp_async_word(kbuf + v * T + t, krow + kbase + v * KT);
+            cp_async_word(kbuf + N + v * T + t, krow + N + kbase + v * KT);
+          }
+          cp_async_commit();
+        } else if constexpr (sizeof(W) == 8) {
+          // Goldilocks keys (191-310 MB) exceed L2: start the key row's way from HBM into L2 while
+          // the digit transform runs (the loads below come after the transform's barriers)
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(krow + kbase + v * KT));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(krow + N + kbase + v * KT));
+          }
+        }
         W x[V];
         if (KSC && ks) {
           // chunk c of the permuted -acc.a (fhe_core/src/key_switch/rlwe.rs:123-131), word u at
@@ -1122,20 +1163,6 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
         } else {
           digits<W, V, T>(x, s_e + part * N, t, j * bits, mask);
         }
-        const W *k = ks     ? p.ksk + (size_t)d * 2 * N
-                     : TERN ? p.bsk + ((((size_t)ph * 2 + br_pair) * 2 + part) * L + j) * 2 * N
-                            : p.bsk + ((size_t)(ph * 2 + part) * L + j) * 2 * N;
-        // Goldilocks keys (191-310 MB) exceed L2: start the key row's way from HBM into L2 while the
-        // digit transform runs (the loads below come after the transform's barriers, so they cannot
-        // be issued earlier). Measured for the Goldilocks sets; BabyBear's 48 MB key stays in L2,
-        // where it only cost instructions, so the 32-bit sets go without it.
-        if constexpr (sizeof(W) == 8) {
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(k + v * T + t));
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(k + N + v * T + t));
-          }
-        }
         NT::forward_small(x, xbuf, ping, s_tw, t, sync);
         if (fold_due_n<FA::FOLD>(nprod)) {
 #pragma unroll
@@ -1144,10 +1171,19 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
             FA::fold(ay[v]);
           }
         }
+        if constexpr (KST) {
+          cp_async_wait_all();
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          FA::mac(ax[v], x[v], k[v * T + t]);
-          FA::mac(ay[v], x[v], k[N + v * T + t]);
+          for (int v = 0; v < V; ++v) {
+            FA::mac(ax[v], x[v], kbuf[v * T + t]);
+            FA::mac(ay[v], x[v], kbuf[N + v * T + t]);
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            FA::mac(ax[v], x[v], krow[kbase + v * KT]);
+            FA::mac(ay[v], x[v], krow[N + kbase + v * KT]);
+          }
         }
         ++nprod;
       }

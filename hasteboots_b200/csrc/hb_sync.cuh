@@ -62,4 +62,16 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// Per-thread asynchronous copy of one 4- or 8-byte word global -> shared (cp.async, L1-allocating):
+// the issuing thread sees it after cp_async_wait_all (the copies of a thread complete in its own
+// order of waits; no other thread may read the word without a barrier after that wait).
+template <class W>
+__device__ __forceinline__ void cp_async_word(W *dst, const W *src) {
+  static_assert(sizeof(W) == 4 || sizeof(W) == 8, "cp.async copies 4 or 8 bytes here");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(sizeof(W))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 }  // namespace hb

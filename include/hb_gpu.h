@@ -159,9 +159,10 @@ int hb_keys_download(hb_ctx *ctx, const hb_keys *keys, void *bsk, size_t bsk_wor
 int hb_gate(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1, const void *c2,
             void *out, size_t count);
 /* Same on device buffers, enqueued on the context stream (one launch per bootstrap layer: MUX takes
- * two). A layer of at most one gate per SM runs the latency form -- one CTA per gate (binary or
- * ternary LWE key), or for the Goldilocks sets a cluster of 4 CTAs per gate -- and larger layers the
- * persistent batched kernel. */
+ * two). A layer of at most one gate per SM runs the latency form -- with a binary LWE key a cluster
+ * of CTAs per gate (4 for the Goldilocks sets, 2 for the 32-bit fields) while the layer holds at
+ * most one cluster CTA per SM, else one CTA per gate -- and larger layers the persistent batched
+ * kernel. */
 int hb_gate_device(hb_ctx *ctx, hb_keys *keys, int gate, const void *c0, const void *c1,
                    const void *c2, void *out, size_t count);
 /* The plain form: one kernel launch per gate. */
