@@ -115,7 +115,9 @@ int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
     psi = chosen;
   }
   const W psi_inv = hb::host_powmod<F>(psi, order - 1);
-  std::vector<W> pw(N), ipw(N), tw(N, 0), itw(N, 0);
+  using Tw = typename F::Tw;  // the twiddle (and for the 32-bit fields its Shoup quotient)
+  std::vector<W> pw(N), ipw(N);
+  std::vector<Tw> tw(N, F::make_tw(0)), itw(N, F::make_tw(0));
   W a = 1, b = 1;
   for (uint32_t i = 0; i < N; ++i) {
     pw[i] = a;
@@ -143,7 +145,7 @@ int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
       const uint32_t rb = bb - lo;
       const uint32_t K = V >> (rb + 1), highs = (1u << s) / K;
       for (uint32_t i = 0; i < (1u << s); ++i)
-        tw[(1u << s) + (i % K) * highs + i / K] = F::to_mont(pw[brv((1u << s) + i, logn)]);
+        tw[(1u << s) + (i % K) * highs + i / K] = F::make_tw(pw[brv((1u << s) + i, logn)]);
     }
     // inverse stage on bit bb: blocks i in [0, H), twiddle psi^-brv(H + i)
     {
@@ -153,21 +155,21 @@ int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
       const uint32_t rb = bb - lo;
       const uint32_t K = V >> (rb + 1), highs = H / K;
       for (uint32_t i = 0; i < H; ++i)
-        itw[H + (i % K) * highs + i / K] = F::to_mont(ipw[brv(H + i, logn)]);
+        itw[H + (i % K) * highs + i / K] = F::make_tw(ipw[brv(H + i, logn)]);
     }
   }
   if (F::RADIX8 && logv == 3) {
     // Radix-8 passes (GroupNtt::fwd_r8 / inv_r8): every forward pass but the first, and every
     // inverse pass, that spans three stages holds theta_m^k (theta_m^-k) at 2^S0 + (k-1) 2^S0 + m,
     // theta_m = psi^brv(2^(S0+2) + 4m) for the 2^S0 blocks of its first stage S0.
-    auto fill = [&](std::vector<W> &tab, uint32_t s0, bool inverse) {
+    auto fill = [&](std::vector<Tw> &tab, uint32_t s0, bool inverse) {
       const uint32_t blocks = 1u << s0;
       for (uint32_t m = 0; m < blocks; ++m) {
         const uint32_t e = brv((1u << (s0 + 2)) + 4 * m, logn);
         const W th = inverse ? ipw[e] : pw[e];
         W pk = th;
         for (uint32_t k = 1; k < 8; ++k) {
-          tab[blocks + (k - 1) * blocks + m] = pk;
+          tab[blocks + (k - 1) * blocks + m] = F::make_tw(pk);
           pk = hb::host_mulmod<F>(pk, th);
         }
       }
@@ -181,15 +183,15 @@ int build_tables(hb_ctx *ctx, uint32_t logn, uint32_t logv, DevTables &t) {
   t.key_scale = F::to_mont(F::to_mont(ninv));
   if (sizeof(W) == 8) t.key_scale = ninv;
   void *dtw = nullptr, *ditw = nullptr;
-  int rc = dev_alloc(ctx, sizeof(W) * N, &dtw);
+  int rc = dev_alloc(ctx, sizeof(Tw) * N, &dtw);
   if (rc) return rc;
-  rc = dev_alloc(ctx, sizeof(W) * N, &ditw);
+  rc = dev_alloc(ctx, sizeof(Tw) * N, &ditw);
   if (rc) {
     dev_free(ctx, dtw);
     return rc;
   }
-  cudaMemcpy(dtw, tw.data(), sizeof(W) * N, cudaMemcpyHostToDevice);
-  cudaMemcpy(ditw, itw.data(), sizeof(W) * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dtw, tw.data(), sizeof(Tw) * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(ditw, itw.data(), sizeof(Tw) * N, cudaMemcpyHostToDevice);
   t.tw = dtw;
   t.itw = ditw;
   return HB_OK;
@@ -283,7 +285,7 @@ int launch_prepare(hb_ctx *ctx, const void *d_in, void *d_out, size_t npolys) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   auto kern = hb::prepare_polys_kernel<F, LOGN, T>;
-  const size_t smem = sizeof(W) * (N + 2 * 2 * N);
+  const size_t smem = sizeof(W) * (hb::tw_words<W>() * N + 2 * 2 * N);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const unsigned grid = (unsigned)std::min<size_t>((npolys + 1) / 2, (size_t)ctx->sms * 4);
   kern<<<std::max(1u, grid), 2 * T, smem, ctx->stream>>>((const W *)d_in, (W *)d_out, npolys,
@@ -320,7 +322,7 @@ int launch_ntt(hb_ctx *ctx, const void *in, void *out, size_t count, int mode) {
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   auto kern = hb::ntt_batch_kernel<F, LOGN, T, GPB>;
-  const size_t smem = sizeof(W) * (2 * N + GPB * 2 * N);
+  const size_t smem = sizeof(W) * (2 * hb::tw_words<W>() * N + GPB * 2 * N);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, GPB * T, smem);
@@ -355,7 +357,7 @@ int launch_ext(hb_ctx *ctx, const void *rgsw, uint32_t bits, uint32_t len, const
   using W = typename F::W;
   constexpr int N = 1 << LOGN;
   auto kern = hb::ext_product_kernel<F, LOGN, T, G, kStages>;
-  const size_t smem = sizeof(W) * (2 * N + kStages * 2 * N + G * 2 * N) + sizeof(uint64_t) * kStages +
+  const size_t smem = sizeof(W) * (2 * hb::tw_words<W>() * N + kStages * 2 * N + G * 2 * N) + sizeof(uint64_t) * kStages +
                       2 * sizeof(uint32_t) * kStages + 16;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const size_t batches = (count + G - 1) / G;
@@ -1164,7 +1166,7 @@ int launch_keygen(hb_ctx *ctx, hb::KeygenParams<typename F::W> &prm) {
   prm.itw = (const W *)tb->itw;
   prm.scale = (W)tb->key_scale;
   auto kern = hb::keygen_rows_kernel<F, LOGN, T>;
-  const size_t smem = sizeof(W) * (2 * N + 2 * 2 * N);
+  const size_t smem = sizeof(W) * (2 * hb::tw_words<W>() * N + 2 * 2 * N);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((prm.rows + 1) / 2, (size_t)ctx->sms * 4));
   kern<<<grid, 2 * T, smem, ctx->stream>>>(prm);

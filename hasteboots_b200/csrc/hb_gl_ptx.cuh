@@ -1,8 +1,9 @@
 // hb_gl_ptx.cuh -- Goldilocks arithmetic written with PTX carry chains so that carries and borrows
-// come from the add/sub instructions themselves instead of 64-bit compares and selects (the
-// bootstrapping kernels are bound by the 32-bit integer ALU, where every 64-bit compare/select
-// costs several instructions). All functions accept any 64-bit word as a representative of its
-// residue mod Q = 2^64 - 2^32 + 1.
+// come from the add/sub instructions themselves instead of 64-bit compares and selects. The
+// bootstrapping kernels are bound by the multiply pipe (ncu: sm__pipe_fmaheavy_cycles_active 81 %
+// against 59 % for the ALU on the 16384-gate GOLDILOCKS launch), so multiplies are kept for the
+// products themselves: multiplications by 2^32 - 1 and the carry corrections are ALU carry chains.
+// All functions accept any 64-bit word as a representative of its residue mod Q = 2^64 - 2^32 + 1.
 #pragma once
 
 #include <cstdint>
@@ -15,21 +16,38 @@ constexpr uint64_t P = 0xFFFFFFFF00000001ULL;
 __device__ __forceinline__ void split(uint64_t x, uint32_t &lo, uint32_t &hi) {
   asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(x));
 }
-// 2^32 - 1 in constant memory: a value the compiler cannot fold, so that 2^32 - 1 - x (~x) can be
-// formed as x (2^32 - 1) + (2^32 - 1) on the multiply pipe instead of the busier logic pipe.
-static __constant__ uint32_t kAllOnes = 0xFFFFFFFFu;
-__device__ __forceinline__ uint32_t not_fma(uint32_t x) {
-  uint32_t r;
-  const uint32_t m = kAllOnes;
-  asm("mad.lo.u32 %0, %1, %2, %2;" : "=r"(r) : "r"(x), "r"(m));
-  return r;
-}
-
 __device__ __forceinline__ uint64_t join(uint32_t lo, uint32_t hi) {
   uint64_t x;
   asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "r"(lo), "r"(hi));
   return x;
 }
+
+// A = x2 (2^32 - 1) + (2^32 - 1 - x3) = x2 2^32 + (2^32 - 1 - x3) - x2 for 32-bit limbs x2, x3
+// (A < 2^64): the low word (2^32 - 1 - x3) - x2, its borrow taken from x2. On the ALU (a multiply-add
+// x2 (2^32 - 1) + ~x3 with ~x3 also formed on the multiply pipe measured 6.0 % slower on 16384
+// GOLDILOCKS gates, 1925.2 vs 1809.5 ms: the multiply pipe is the bound one).
+__device__ __forceinline__ uint64_t fold_hi(uint32_t x2, uint32_t x3) {
+  uint32_t a0, a1;
+  asm("sub.cc.u32 %0, %2, %3;\n\t"
+      "subc.u32   %1, %3, 0;"
+      : "=&r"(a0), "=r"(a1)
+      : "r"(~x3), "r"(x2));
+  return join(a0, a1);
+}
+// z (2^32 - 1) = z 2^32 - z as limbs: low word -z, its borrow (z != 0) taken from z (two ALU
+// instructions instead of a wide multiply: 1788.6 -> 1780.1 ms on 16384 GOLDILOCKS gates).
+__device__ __forceinline__ void times_eps(uint32_t z, uint32_t &lo, uint32_t &hi) {
+  asm("sub.cc.u32 %0, 0, %2;\n\t"
+      "subc.u32   %1, %2, 0;"
+      : "=&r"(lo), "=r"(hi)
+      : "r"(z));
+}
+// c (2^32 - 1) for a carry c in {0, 1}, added to (r0, r1) with carry: -c in the low word (an ALU
+// negation instead of two multiply-adds c (2^32 - 1): with fold_hi's ALU form, 1809.5 -> 1789.2 ms).
+#define HB_GL_ADD_EPS_C \
+  "neg.s32        c, c;\n\t" \
+  "add.cc.u32     %0, %0, c;\n\t" \
+  "addc.u32       %1, %1, 0;\n\t"
 
 // a * b folded to [0, 2^64) (not necessarily canonical).
 // Product limbs x0..x3, then x = lo + x2 2^64 + x3 2^96 = lo + x2 (2^32 - 1) - x3 (mod Q):
@@ -51,8 +69,7 @@ __device__ __forceinline__ uint64_t mul_lazy(uint64_t a, uint64_t b) {
       "addc.u32       %3, %3, 0;"
       : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
       : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-  uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
+  const uint64_t A = fold_hi(x2, x3);
   uint32_t A0, A1;
   split(A, A0, A1);
   uint32_t r0, r1;
@@ -99,22 +116,17 @@ __device__ __forceinline__ uint64_t reduce_canon_lo(uint32_t x0, uint32_t x1, ui
   return join(r0, r1);
 }
 __device__ __forceinline__ uint64_t reduce_canon(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
-  uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
-  return reduce_canon_lo(x0, x1, A);
+  return reduce_canon_lo(x0, x1, fold_hi(x2, x3));
 }
-// reduce_canon with x3 = 0: A = x2 (2^32 - 1) + (2^32 - 1) in one multiply-add.
+// reduce_canon with x3 = 0: A = x2 (2^32 - 1) + (2^32 - 1) = x2 2^32 + (2^32 - 1 - x2), no borrow.
 __device__ __forceinline__ uint64_t reduce_canon_x3zero(uint32_t x0, uint32_t x1, uint32_t x2) {
-  uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, 0xFFFFFFFF;" : "=l"(A) : "r"(x2));
-  return reduce_canon_lo(x0, x1, A);
+  return reduce_canon_lo(x0, x1, join(~x2, x2));
 }
 
 // reduce_canon with x0 = 0: the low limb of lo + A is A0 and cannot carry (one instruction fewer
 // than reduce_canon; with the x3 = 0 form above, 1.0 % off the bootstrapping kernel).
 __device__ __forceinline__ uint64_t reduce_canon_x0zero(uint32_t x1, uint32_t x2, uint32_t x3) {
-  uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
+  const uint64_t A = fold_hi(x2, x3);
   uint32_t A0, A1;
   split(A, A0, A1);
   uint32_t r0, r1;
@@ -161,8 +173,7 @@ __device__ __forceinline__ void mac_lazy(uint64_t &acc, uint32_t &cnt, uint64_t 
       "addc.u32       %3, %3, 0;"
       : "=&r"(x0), "=&r"(x1), "=&r"(x2), "=&r"(x3)
       : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-  uint64_t A;
-  asm("mad.wide.u32 %0, %1, 0xFFFFFFFF, %2;" : "=l"(A) : "r"(x2), "l"((uint64_t)not_fma(x3)));
+  const uint64_t A = fold_hi(x2, x3);
   uint32_t A0, A1, c0, c1;
   split(A, A0, A1);
   split(acc, c0, c1);
@@ -201,10 +212,8 @@ __device__ __forceinline__ uint64_t mul_pow2(uint64_t y) {
     const uint64_t H = y >> (96 - E);
     uint32_t h0, h1;
     split(H, h0, h1);
-    uint64_t A;
-    asm("mul.wide.u32 %0, %1, 0xFFFFFFFF;" : "=l"(A) : "r"(z));
     uint32_t A0, A1;
-    split(A, A0, A1);
+    times_eps(z, A0, A1);
     uint32_t d0, d1;
     asm("{\n\t.reg .u32 bw;\n\t"
         "sub.cc.u32  %0, %2, %4;\n\t"
@@ -226,8 +235,7 @@ __device__ __forceinline__ uint64_t canon(uint64_t r) {
       "add.cc.u32     t0, %0, 0xFFFFFFFF;\n\t"
       "addc.cc.u32    t1, %1, 0;\n\t"
       "addc.u32       c, 0, 0;\n\t"
-      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %0;\n\t"
-      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t}"
+      HB_GL_ADD_EPS_C "}"
       : "+r"(r0), "+r"(r1));
   return join(r0, r1);
 }
@@ -244,8 +252,7 @@ __device__ __forceinline__ uint64_t add_c(uint64_t a, uint64_t b) {
       "add.cc.u32     %0, %2, %4;\n\t"
       "addc.cc.u32    %1, %3, %5;\n\t"
       "addc.u32       c, 0, 0;\n\t"
-      "mad.lo.cc.u32  %0, c, 0xFFFFFFFF, %0;\n\t"
-      "madc.hi.u32    %1, c, 0xFFFFFFFF, %1;\n\t}"
+      HB_GL_ADD_EPS_C "}"
       : "=&r"(s0), "=&r"(s1)
       : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
   return join(s0, s1);
@@ -272,8 +279,9 @@ __device__ __forceinline__ uint64_t sub_c(uint64_t a, uint64_t b) {
 // off = Q - m (2^32 - 1) removes the offsets of the m products (cnt (2^32 - 1) < 2^38 and off < Q,
 // so both additions take the one-carry form).
 __device__ __forceinline__ uint64_t mac_lazy_value(uint64_t acc, uint32_t cnt, uint64_t off) {
-  uint64_t t;
-  asm("mul.wide.u32 %0, %1, 0xFFFFFFFF;" : "=l"(t) : "r"(cnt));
+  uint32_t t0, t1;
+  times_eps(cnt, t0, t1);
+  const uint64_t t = join(t0, t1);
   return add_c(add_c(acc, t), off);
 }
 

@@ -161,10 +161,11 @@ __global__ void __launch_bounds__(2 * T) prepare_polys_kernel(const typename F::
   using NT = GroupNtt<F, LOGN, T>;
   constexpr int N = 1 << LOGN, V = NT::V;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int TWN = N * F::TW_WORDS;  // words of a twiddle table
   W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_x = s_tw + N;
+  W *s_x = s_tw + TWN;
   const int g = threadIdx.x / T, t = threadIdx.x % T;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) s_tw[i] = tw_g[i];
+  for (int i = threadIdx.x; i < TWN; i += blockDim.x) s_tw[i] = tw_g[i];
   __syncthreads();
   GroupSync<T> sync{1 + g};
   W *xbuf = s_x + g * 2 * N;
@@ -215,11 +216,12 @@ __global__ void __launch_bounds__(GPB * T) ntt_batch_kernel(const typename F::W 
   using NT = GroupNtt<F, LOGN, T>;
   constexpr int N = 1 << LOGN, V = NT::V;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int TWN = N * F::TW_WORDS;
   W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_itw = s_tw + N;
-  W *s_x = s_itw + N;
+  W *s_itw = s_tw + TWN;
+  W *s_x = s_itw + TWN;
   const int g = threadIdx.x / T, t = threadIdx.x % T;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+  for (int i = threadIdx.x; i < TWN; i += blockDim.x) {
     s_tw[i] = tw_g[i];
     s_itw[i] = itw_g[i];
   }
@@ -345,16 +347,17 @@ __global__ void __launch_bounds__(G * T, 1)
   using NT = GroupNtt<F, LOGN, T>;
   constexpr int N = 1 << LOGN, V = NT::V;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int TWN = N * F::TW_WORDS;
   W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_itw = s_tw + N;
-  W *s_k = s_itw + N;
+  W *s_itw = s_tw + TWN;
+  W *s_k = s_itw + TWN;
   W *s_x = s_k + S * 2 * N;
   uint64_t *s_bar = reinterpret_cast<uint64_t *>(s_x + G * 2 * N);
   uint32_t *s_cnt = reinterpret_cast<uint32_t *>(s_bar + S);
   uint32_t *s_issued = s_cnt + S;
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_issued + S);
   const int tid = threadIdx.x, g = tid / T, t = tid % T;
-  for (int i = tid; i < N; i += blockDim.x) {
+  for (int i = tid; i < TWN; i += blockDim.x) {
     s_tw[i] = tw_g[i];
     s_itw[i] = itw_g[i];
   }
@@ -499,8 +502,8 @@ constexpr int kBootXbuf = kBootPingPong ? 2 : 1;  // exchange buffers of N words
 
 template <class W, int N, int G, int S>
 __host__ __device__ constexpr size_t boot_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(2 * N + S * 2 * N + G * (3 + kBootXbuf) * N) + sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) +
-         sizeof(uint64_t) * S + 2 * sizeof(uint32_t) * S + 16;
+  return sizeof(W) * (size_t)(2 * tw_words<W>() * N + S * 2 * N + G * (3 + kBootXbuf) * N) +
+         sizeof(uint16_t) * (size_t)G * ((n + 8) & ~7u) + sizeof(uint64_t) * S + 2 * sizeof(uint32_t) * S + 16;
 }
 
 // Key-chunk stages of a bootstrap_kernel variant: 3 when they fit the 227 KB of shared memory a
@@ -523,11 +526,11 @@ template <class F, int LOGN, int T, int G, int S, bool TERN = false, bool KSC = 
 __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T, kBootPingPong>;
-  constexpr int N = 1 << LOGN, V = NT::V;
+  constexpr int N = 1 << LOGN, V = NT::V, TWN = N * F::TW_WORDS;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_itw = s_tw + N;
-  W *s_k = s_itw + N;
+  W *s_itw = s_tw + TWN;
+  W *s_k = s_itw + TWN;
   W *s_grp = s_k + S * 2 * N;
   W *s_e = s_grp + G * (2 + kBootXbuf) * N;
   const uint32_t msz = (p.n + 8) & ~7u;
@@ -538,7 +541,7 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_issued + S);
 
   const int tid = threadIdx.x, g = tid / T, t = tid % T;
-  for (int i = tid; i < N; i += blockDim.x) {
+  for (int i = tid; i < TWN; i += blockDim.x) {
     s_tw[i] = p.tw[i];
     s_itw[i] = p.itw[i];
   }
@@ -919,14 +922,15 @@ __host__ __device__ constexpr int dp_wide_words() {
   return N / (dp_groups<W, KT, C>() / 2 * dp_group_threads<W, KT, C>());
 }
 
-// Shared memory of bootstrap_dp_kernel: twiddles (2N words: forward, inverse of the half-CTA
-// layout), the accumulator (2N), the decomposition sources E.a and E.b (2N), per group two exchange
+// Shared memory of bootstrap_dp_kernel: twiddle tables (forward, inverse of the half-CTA layout;
+// N entries each), the accumulator (2N), the decomposition sources E.a and E.b (2N), per group two exchange
 // buffers (2N) that also carry the group's partial sums, with KST the key words of its digit (2N), in a
 // cluster two buffers of the CTA's partial sums that the other CTAs read (2 x 2N), and the
 // modulus-switched input.
 template <class W, int N, int D, int C, bool KST>
 __host__ __device__ constexpr size_t dp_smem_bytes(uint32_t n) {
-  return sizeof(W) * (size_t)(6 + (KST ? 4 : 2) * D + (C > 1 ? 4 : 0)) * N + sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
+  return sizeof(W) * (size_t)(2 * tw_words<W>() + 4 + (KST ? 4 : 2) * D + (C > 1 ? 4 : 0)) * N +
+         sizeof(uint16_t) * (size_t)((n + 8) & ~7u);
 }
 
 // Cluster barrier halves (all threads of every CTA of the cluster, warp-uniform): arrive releases
@@ -992,9 +996,10 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
   using NW = GroupNtt<F, LOGN, TW>;
   constexpr int VW = NW::V;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int TWN = N * F::TW_WORDS;
   W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_itw_w = s_tw + N;
-  W *acc_a = s_itw_w + N;
+  W *s_itw_w = s_tw + TWN;
+  W *acc_a = s_itw_w + TWN;
   W *acc_b = acc_a + N;
   W *s_e = acc_b + N;  // E.a then E.b (the key switch: -acc.a), natural order
   W *s_x = s_e + 2 * N;
@@ -1009,7 +1014,7 @@ __global__ void __launch_bounds__(D * T, 1) bootstrap_dp_kernel(const BootParams
   const uint32_t rank = C > 1 ? cluster_rank() : 0;
   const int gg = (int)rank * D + g;  // the group's index in the cluster (digits gg, gg + C D, ...)
   uint32_t cp_turn = 0;              // C > 1: which sum buffer this phase writes
-  for (int i = tid; i < N; i += NT_ALL) {
+  for (int i = tid; i < TWN; i += NT_ALL) {
     s_tw[i] = p.tw[i];
     s_itw_w[i] = p.itw_w[i];
   }

@@ -41,13 +41,13 @@ template <class F, int LOGN, int T>
 __global__ void __launch_bounds__(2 * T) keygen_rows_kernel(const KeygenParams<typename F::W> p) {
   using W = typename F::W;
   using NT = GroupNtt<F, LOGN, T>;
-  constexpr int N = 1 << LOGN, V = NT::V;
+  constexpr int N = 1 << LOGN, V = NT::V, TWN = N * F::TW_WORDS;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   W *s_tw = reinterpret_cast<W *>(smem_raw);
-  W *s_itw = s_tw + N;
-  W *s_x = s_itw + N;
+  W *s_itw = s_tw + TWN;
+  W *s_x = s_itw + TWN;
   const int g = threadIdx.x / T, t = threadIdx.x % T;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+  for (int i = threadIdx.x; i < TWN; i += blockDim.x) {
     s_tw[i] = p.tw[i];
     s_itw[i] = p.itw[i];
   }

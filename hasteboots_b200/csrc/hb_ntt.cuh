@@ -20,6 +20,13 @@ namespace hb {
 
 __host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x >> 1); }
 
+// Words per entry of a twiddle table for word type W: the 32-bit fields keep a Shoup quotient
+// beside each twiddle (Mont32::Tw), Goldilocks the twiddle alone.
+template <class W>
+__host__ __device__ constexpr int tw_words() {
+  return sizeof(W) == 4 ? 2 : 1;
+}
+
 // Synchronisation of one thread group: a warp (T == 32) or a named barrier (T > 32).
 template <int T>
 struct GroupSync {
@@ -38,6 +45,9 @@ struct GroupSync {
 template <class F, int LOGN, int T, bool PP = true>
 struct GroupNtt {
   using W = typename F::W;
+  using TwT = typename F::Tw;  // table entry: F::TW_WORDS words (the 32-bit fields add a Shoup quotient)
+  static constexpr int TW_WORDS = F::TW_WORDS;
+  static_assert(TW_WORDS == tw_words<W>() && sizeof(TwT) == TW_WORDS * sizeof(W), "twiddle entry layout");
   static constexpr int N = 1 << LOGN;
   static constexpr int V = N / T;
   static constexpr int LOGV = ilog2c(V);
@@ -75,10 +85,10 @@ struct GroupNtt {
     for (int v = 0; v < V; ++v) x[v] = buf[pt ^ cphys(v << LO_TO)];
   }
 
-  // Twiddle tables are stored stage by stage; within the 2^S entries of a stage, entry
-  // high * K + k (the k-th distinct twiddle of the threads whose bits above the pass are `high`)
-  // sits at high + k * (2^S / K), so the loads of a warp are broadcasts or consecutive words
-  // (build_tables in hb_api.cu writes this layout).
+  // Twiddle tables (N entries of F::Tw, N * F::TW_WORDS words) are stored stage by stage; within
+  // the 2^S entries of a stage, entry high * K + k (the k-th distinct twiddle of the threads whose
+  // bits above the pass are `high`) sits at high + k * (2^S / K), so the loads of a warp are
+  // broadcasts or consecutive entries (build_tables in hb_api.cu writes this layout).
 
   __host__ __device__ static constexpr int brvc(int x, int bits) {
     int r = 0;
@@ -199,7 +209,7 @@ struct GroupNtt {
       const int base = (1 << S) + (t >> LO);
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        const W w = tw[base + k * HIGHS];
+        const TwT w = reinterpret_cast<const TwT *>(tw)[base + k * HIGHS];
 #pragma unroll
         for (int l = 0; l < (1 << RB); ++l) {
           const int v = (k << (RB + 1)) | l;
@@ -218,7 +228,7 @@ struct GroupNtt {
     const int base = H + (t >> LO);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const W w = itw[base + k * HIGHS];
+      const TwT w = reinterpret_cast<const TwT *>(itw)[base + k * HIGHS];
 #pragma unroll
       for (int l = 0; l < (1 << RB); ++l) {
         const int v = (k << (RB + 1)) | l;

@@ -17,8 +17,8 @@ struct GateJob;
 namespace hbrt {
 
 struct DevTables {
-  void *tw = nullptr;   // psi^brv(k) (Montgomery form for BabyBear)
-  void *itw = nullptr;  // psi^-brv(k)
+  void *tw = nullptr;   // N entries of F::Tw: psi^brv(k) (the 32-bit fields: with its Shoup quotient)
+  void *itw = nullptr;  // psi^-brv(k), the same way
   unsigned long long n_inv = 0;      // multiplier giving x * N^-1
   unsigned long long key_scale = 0;  // multiplier applied to key words at upload
 };
