@@ -1,8 +1,9 @@
-"""The 32-bit fields' multiply-accumulate (hasteboots_b200/csrc/hb_field.cuh, Mont32::Acc) compiled
-for the host with g++ and checked against exact integer arithmetic: DefaultFieldU32's 64-bit
-unreduced sums with residue-keeping folds (forced here at every spacing up to FOLD, and at the
-extreme word values), and BabyBear's per-product reduction. The value of a sum of products x k is
-sum(x k) 2^-32 mod P, since the keys it multiplies are stored in Montgomery form."""
+"""The 32-bit fields' arithmetic (hasteboots_b200/csrc/hb_field.cuh, Mont32) compiled for the host
+with g++ and checked against exact integer arithmetic: the multiply-accumulate (DefaultFieldU32's
+64-bit unreduced sums with residue-keeping folds, forced here at every spacing up to FOLD and at the
+extreme word values, and BabyBear's per-product reduction; the value of a sum of products x k is
+sum(x k) 2^-32 mod P, since the keys it multiplies are stored in Montgomery form), and the Shoup
+twiddle product and butterflies of the NTT tables (Mont32::make_tw, shoup, ct, gs)."""
 
 import os
 import random
@@ -34,7 +35,25 @@ void run() {
     printf("%u\n", (unsigned)F::acc_value(a, 0));
   }
 }
+template <class F>
+void run_shoup() {
+  using W = typename F::W;
+  unsigned a, w, x, y;
+  // "a w x y": shoup(a, w) and the CT / GS butterflies of (x, y) with twiddle w
+  while (scanf("%u %u %u %u", &a, &w, &x, &y) == 4) {
+    const typename F::Tw t = F::make_tw((W)w);
+    W cx = (W)x, cy = (W)y, gx = (W)x, gy = (W)y;
+    F::ct(cx, cy, t);
+    F::gs(gx, gy, t);
+    printf("%u %u %u %u %u\n", (unsigned)F::shoup((W)a, t.w, t.q), (unsigned)cx, (unsigned)cy, (unsigned)gx,
+           (unsigned)gy);
+  }
+}
 int main(int argc, char **argv) {
+  if (argv[1][0] == 's') {
+    if (argv[1][1] == 'd') run_shoup<hb::DefaultFieldU32>(); else run_shoup<hb::BabyBear>();
+    return 0;
+  }
   if (argv[1][0] == 'd') run<hb::DefaultFieldU32>(); else run<hb::BabyBear>();
   printf("FOLD %d\n", argv[1][0] == 'd' ? hb::DefaultFieldU32::FOLD : hb::BabyBear::FOLD);
   return 0;
@@ -77,3 +96,23 @@ def test_accumulate_matches_exact_sums(driver, field, P):
         assert int(got) == expect, (n, fold)
     if field == "d":
         assert fold_max >= 27  # DEFAULT_TERNARY's key switch sums 27 products without a fold
+
+
+@pytest.mark.parametrize("field,P", [("d", 132120577), ("b", 0x78000001)])
+def test_shoup_twiddle_products_are_exact(driver, field, P):
+    rng = random.Random(11)
+    M = 1 << 32
+    cases = [(rng.randrange(M), rng.randrange(P), rng.randrange(P), rng.randrange(P)) for _ in range(4000)]
+    for a in (0, 1, P - 1, P, M - 1):
+        for w in (0, 1, P - 1):
+            cases.append((a, w, P - 1, P - 1))
+            cases.append((a, w, 0, P - 1))
+    text = "".join(f"{a} {w} {x} {y}\n" for a, w, x, y in cases)
+    out = subprocess.run([driver, "s" + field], input=text, capture_output=True, text=True, check=True).stdout.split("\n")
+    for (a, w, x, y), line in zip(cases, out):
+        r, cx, cy, gx, gy = map(int, line.split())
+        assert r == a * w % P, (a, w)
+        # CT: (x + w y, x - w y); GS: (x + y, (x - y) w), canonical
+        assert (cx, cy) == ((x + w * y) % P, (x - w * y) % P), (x, y, w)
+        assert (gx, gy) == ((x + y) % P, (x - y) * w % P), (x, y, w)
+
