@@ -1,8 +1,9 @@
 // hb_gl_ptx.cuh -- Goldilocks arithmetic written with PTX carry chains so that carries and borrows
-// come from the add/sub instructions themselves instead of 64-bit compares and selects. The
-// bootstrapping kernels are bound by the multiply pipe (ncu: sm__pipe_fmaheavy_cycles_active 81 %
-// against 59 % for the ALU on the 16384-gate GOLDILOCKS launch), so multiplies are kept for the
-// products themselves: multiplications by 2^32 - 1 and the carry corrections are ALU carry chains.
+// come from the add/sub instructions themselves instead of 64-bit compares and selects.
+// Multiplies are kept for the products themselves: multiplications by 2^32 - 1 and the carry
+// corrections are ALU carry chains. With them as multiply-adds the bootstrapping kernel was bound by
+// the integer multiply-add pipe (ncu: sm__pipe_fmaheavy_cycles_active 81 % against 59 % for the
+// ALU); with the ALU forms the two read 69 % and 76 % and the launch is 7.5 % shorter.
 // All functions accept any 64-bit word as a representative of its residue mod Q = 2^64 - 2^32 + 1.
 #pragma once
 
