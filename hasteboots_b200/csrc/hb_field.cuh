@@ -153,6 +153,11 @@ struct Goldilocks {
     a.cnt = 0;
   }
   __device__ __forceinline__ static void acc_mac(Acc &a, W x, W k) { glx::mac_lazy(a.lo, a.cnt, x, k); }
+  __device__ __forceinline__ static void acc_mac2(Acc &a, W x, W kx, W y, W ky) {
+    glx::mac_lazy(a.lo, a.cnt, x, kx);
+    glx::mac_lazy(a.lo, a.cnt, y, ky);
+  }
+  static constexpr bool WIDE = false;  // products accumulate lazily in 96 bits, not as 64-bit sums
   // The carry count never overflows for the sums here (at most 2^32 products): no folds.
   static constexpr int FOLD = 1 << 30;
   __device__ __forceinline__ static void acc_fold(Acc &) {}
@@ -296,6 +301,17 @@ struct Mont32 {
       a.t += (uint64_t)x * k;
     } else {
       a.t = mac(a.t, x, k);
+    }
+  }
+  // a += x kx + y ky. Per-product reduction (BabyBear): the two products share one Montgomery
+  // reduction, since x kx + y ky < 2 P^2 < P 2^32 (2P < 2^32) keeps it below 2P.
+  HB_HD static void acc_mac2(Acc &a, W x, W kx, W y, W ky) {
+    if constexpr (WIDE) {
+      a.t += (uint64_t)x * kx;
+      a.t += (uint64_t)y * ky;
+    } else {
+      const uint64_t t = (uint64_t)x * kx + (uint64_t)y * ky;
+      a.t = add(a.t, canon((W)redc_lazy(t)));
     }
   }
   HB_HD static void acc_fold(Acc &a) {

@@ -111,6 +111,20 @@ struct GroupPipe {
     }
     return stages + st * WORDS;
   }
+  // The chunk after the current one, held together with it (two releases follow). Cannot deadlock
+  // with S >= 2: that chunk's copy waits only on the releases of chunk next + 1 - S, which every
+  // group passed before it took chunk next.
+  __device__ __forceinline__ const W *acquire_next() {
+    static_assert(S >= 2, "two chunks held at once need two stages");
+    const unsigned long long c = next + 1;
+    const int st = (int)(c % S);
+    const uint32_t par = (uint32_t)((c / S) & 1);
+    if (!mbar_wait_bounded(&bars[st], par, budget)) {
+      *abort_flag = 1;
+      atomicOr(status, STATUS_TIMEOUT);
+    }
+    return stages + st * WORDS;
+  }
   // Group-wide release of the current chunk (t: the thread's index in its group); false when the
   // launch must stop.
   template <class Src, class Sync>
@@ -748,6 +762,23 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
         }
         return true;
       };
+      // DUAL, binary key: two transformed digits against their consecutive key chunks, held at once;
+      // the two products of a slot share one reduction (F::acc_mac2; BABYBEAR 16384 gates, same GPU:
+      // T = 64, G = 8 352.6 -> 341.8 ms, T = 128, G = 4 416.1 -> 395.4 ms)
+      auto mac_pair = [&](W(&x)[V], W(&y)[V]) -> bool {
+        const W *k0 = pipe.acquire();
+        const W *k1 = pipe.acquire_next();
+        if (active) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            F::acc_mac2(acc_x[v], x[v], k0[v * T + t], y[v], k1[v * T + t]);
+            F::acc_mac2(acc_y[v], x[v], k0[N + v * T + t], y[v], k1[N + v * T + t]);
+          }
+        }
+        nprod += 2;
+        if (!pipe.release(src, t, sync)) return false;
+        return pipe.release(src, t, sync);
+      };
       // TRACE: digit j of E.part at step ph / 2; coefficient v T + t is in x[v]
       auto trace_digit = [&](const W(&x)[V], uint32_t j) {
         if constexpr (TRACE) {
@@ -770,7 +801,11 @@ __global__ void __launch_bounds__(G * T, 1) bootstrap_kernel(const BootParams<ty
             trace_digit(y, j + 1);
             NT::forward_small2(x, y, xbuf, ping, s_tw, t, sync);
           }
-          if (!mac_digit(x) || !mac_digit(y)) goto aborted;
+          if constexpr (!TERN && !F::WIDE) {
+            if (!mac_pair(x, y)) goto aborted;
+          } else {
+            if (!mac_digit(x) || !mac_digit(y)) goto aborted;
+          }
         }
       }
       for (; j < L; ++j) {

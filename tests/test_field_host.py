@@ -49,7 +49,27 @@ void run_shoup() {
            (unsigned)gy);
   }
 }
+template <class F>
+void run_pairs() {
+  using W = typename F::W;
+  unsigned n;
+  // "n x1 k1 y1 l1 ...": n pair steps a += x k + y l from zero
+  while (scanf("%u", &n) == 1) {
+    typename F::Acc a;
+    F::acc_clear(a);
+    for (unsigned i = 0; i < n; ++i) {
+      unsigned x, k, y, l;
+      if (scanf("%u %u %u %u", &x, &k, &y, &l) != 4) return;
+      F::acc_mac2(a, (W)x, (W)k, (W)y, (W)l);
+    }
+    printf("%u\n", (unsigned)F::acc_value(a, 0));
+  }
+}
 int main(int argc, char **argv) {
+  if (argv[1][0] == 'p') {
+    if (argv[1][1] == 'd') run_pairs<hb::DefaultFieldU32>(); else run_pairs<hb::BabyBear>();
+    return 0;
+  }
   if (argv[1][0] == 's') {
     if (argv[1][1] == 'd') run_shoup<hb::DefaultFieldU32>(); else run_shoup<hb::BabyBear>();
     return 0;
@@ -115,4 +135,22 @@ def test_shoup_twiddle_products_are_exact(driver, field, P):
         # CT: (x + w y, x - w y); GS: (x + y, (x - y) w), canonical
         assert (cx, cy) == ((x + w * y) % P, (x - w * y) % P), (x, y, w)
         assert (gx, gy) == ((x + y) % P, (x - y) * w % P), (x, y, w)
+
+
+@pytest.mark.parametrize("field,P", [("d", 132120577), ("b", 0x78000001)])
+def test_pair_accumulate_matches_exact_sums(driver, field, P):
+    """Mont32::acc_mac2: the two products of a pair share one reduction (BabyBear) or add to the
+    64-bit sum (DefaultFieldU32); value sum(x k + y l) 2^-32 mod P."""
+    rng = random.Random(13)
+    cases = []
+    for n in (1, 2, 4, 7, 13):
+        cases.append([tuple(rng.randrange(P) for _ in range(4)) for _ in range(n)])
+    cases.append([(P - 1, P - 1, P - 1, P - 1)] * 13)
+    cases.append([(P - 1, P - 1, 0, 0), (0, 0, P - 1, P - 1)])
+    text = "".join(f"{len(c)} " + " ".join(" ".join(map(str, q)) for q in c) + "\n" for c in cases)
+    out = subprocess.run([driver, "p" + field], input=text, capture_output=True, text=True, check=True).stdout.split()
+    rinv = pow(1 << 32, -1, P)
+    for c, got in zip(cases, out):
+        expect = sum(x * k + y * l for x, k, y, l in c) * rinv % P
+        assert int(got) == expect, c[:2]
 
